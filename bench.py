@@ -1,0 +1,309 @@
+#!/usr/bin/env python
+"""Benchmark of the FR P=3 step path on B200.
+
+Workload (N=1): the compressible channel at 48^3 elements (7,077,888 solution
+points, 141.6 MB f32 state) on [0,2pi]x[0,2]x[0,pi], slip walls in y,
+SLAU2, f32 pipeline, Mach 0.2 laminar profile + wall-damped Fourier trip
+(amplitude 0.01 = 0.05 U_bulk, 16 modes, seed 42), the reference's physics
+(mu = 1.6e-4, forcing 1e-3). Synthetic: the IC generator builds the state.
+
+One bench "step" is one dump interval of 50 SSP-RK3 time steps (150 stages),
+the cadence of the reference's own 48^3 timings (dumps every 50 steps).
+  value : Gdof*stage/s with the state resident in HBM (CUDA events on the
+          solver's stream, barrier + synchronize on both sides, max over ranks)
+  e2e   : the same through the C ABI with pinned host buffers: every bench
+          step uploads the state (od_set_state), runs the 50 RK3 steps
+          (od_step) and downloads the state (od_get_state)
+The state (141.6 MB per buffer, three buffers) is larger than the 126 MB L2.
+
+--impl reference times the reference's own kernels (compiled from its CUDA
+sources with NVRTC, launched with its launch shapes and sequence) on the same
+GPU and workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(nx=48, ny=48, nz=48, lx=2 * math.pi, ly=2.0, lz=math.pi, mach=0.2, amp=0.01, modes=16, seed=42,
+                flux="slau2", y_wall=True, prec="f32", dt=2e-4)
+RK_PER_STEP = 50
+METRIC = "Gdof*stage/s (48^3 channel, FR P=3, f32, SLAU2)"
+BYTES_PER_DOF_STAGE = 40.0 / 3.0  # x sizeof(state): read u + write u' (stage 1), read u0, u + write (stages 2, 3)
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_state(dtype=np.float32):
+    from opendynamo_b200 import initial_state as ic
+    w = WORKLOAD
+    planes = ic.channel_state(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"], w["lz"], w["mach"], "channel", w["amp"],
+                              w["modes"], w["seed"])
+    return ic.stack(planes, dtype)
+
+
+def cpu_baseline(u: np.ndarray) -> dict:
+    """The project's multithreaded FP64 oracle on this host's cores: one RK3
+    step of the 48^3 channel (a bounded sample of the workload)."""
+    import oracle
+    w = WORKLOAD
+    cores = os.cpu_count() or 1
+    p = oracle.make_params(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"], w["lz"], flux=w["flux"], y_wall=w["y_wall"],
+                           u="f64", threads=cores)
+    u64 = u.astype(np.float64)
+    oracle.lib()
+    t0 = time.perf_counter()
+    oracle.run(p, u64, 1, w["dt"])
+    sec = time.perf_counter() - t0
+    npts = w["nx"] * w["ny"] * w["nz"] * 64
+    return {"value": npts * 3 / sec / 1e9, "unit": "Gdof*stage/s", "cores": cores, "kind": "port",
+            "sample": f"1 SSP-RK3 step (3 stages) of the 48^3 channel in FP64, {sec:.2f} s"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from opendynamo_b200.solver import Solver, make_params
+
+    w = WORKLOAD
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        import datetime
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    u_host = build_state(np.float32)
+    npts = w["nx"] * w["ny"] * w["nz"] * 64
+    params = make_params(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"], w["lz"], w["flux"], w["y_wall"], w["prec"],
+                         device=local)
+    solver = Solver(params)
+    dt = float(np.float32(w["dt"]))
+    stream = torch.cuda.ExternalStream(solver.stream, device=f"cuda:{local}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    solver.set_state(u_host)
+    for _ in range(args.warmup):
+        solver.step(RK_PER_STEP, dt)
+    solver.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        solver.step(RK_PER_STEP, dt)
+    ev1.record(stream)
+    solver.sync()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    stages = args.steps * RK_PER_STEP * 3
+    value = world * npts * stages / (ms / 1e3) / 1e9
+
+    # ---- dominant kernel (phase A) timed live with events on the solver's stream
+    solver.set_timing(True)
+    solver.step(RK_PER_STEP, dt)
+    ms_a, ms_b, n_st = solver.timing()
+    solver.set_timing(False)
+    s_bytes = 4
+    alg_bytes_launch = BYTES_PER_DOF_STAGE * s_bytes * npts
+    avg_a = ms_a / n_st
+    achieved = alg_bytes_launch / (avg_a / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+
+    # ---- e2e through the C ABI with pinned host buffers
+    h_in = torch.from_numpy(u_host).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    lib = solver._lib
+    import ctypes
+    for _ in range(1):
+        N_chk = lib.od_set_state(solver._ctx, ctypes.c_void_p(h_in.data_ptr()), solver.state_bytes)
+        assert N_chk == 0
+        solver.step(RK_PER_STEP, dt)
+        assert lib.od_get_state(solver._ctx, ctypes.c_void_p(h_out.data_ptr()), solver.state_bytes) == 0
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        assert lib.od_set_state(solver._ctx, ctypes.c_void_p(h_in.data_ptr()), solver.state_bytes) == 0
+        solver.step(RK_PER_STEP, dt)
+        assert lib.od_get_state(solver._ctx, ctypes.c_void_p(h_out.data_ptr()), solver.state_bytes) == 0
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * npts * stages / e2e_s / 1e9
+    final = h_out.numpy()
+    finite = bool(np.isfinite(final).all())
+
+    out = None
+    if rank == 0:
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "stage_a_traffic.json")
+        if os.path.exists(tpath):
+            try:
+                with open(tpath) as fh:
+                    traffic = json.load(fh).get("bytes_per_launch")
+            except Exception:
+                traffic = None
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Gdof*stage/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (channel IC generator: laminar profile + Fourier trip, seed 42)",
+            "config": {"workload": "channel 48^3 elements, FR P=3 (7,077,888 dofs), SLAU2, y slip walls, f32",
+                       "rk3_steps_per_step": RK_PER_STEP, "dt": dt, "global_dofs": world * npts,
+                       "l2": "inputs larger than L2 (141.6 MB state x 3 buffers > 126 MB)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Gdof*stage/s",
+                    "h2d_bytes_per_step": int(solver.state_bytes), "d2h_bytes_per_step": int(solver.state_bytes)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "od::stage_a_kernel (phase A, one launch per RK stage)",
+                         "avg_launch_ms": round(avg_a, 5), "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": int(alg_bytes_launch),
+                         "phase_b_avg_ms": round(ms_b / n_st, 5)},
+            "gpu_launches": int(solver.launches_per_step * RK_PER_STEP * args.steps),
+            "clocks": clk,
+            "state_finite": finite,
+            "step_effective_gbs": round(value / world * BYTES_PER_DOF_STAGE * s_bytes, 1),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(u_host)
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return out
+
+
+def run_reference(args, world, rank, local):
+    if rank != 0:
+        return None
+    try:
+        from oracle import ref_harness
+    except Exception as exc:  # pragma: no cover
+        return {"impl": "reference", "unavailable": f"reference harness not importable: {exc}"}
+    return ref_harness.bench_line(args, WORKLOAD, RK_PER_STEP, METRIC, BYTES_PER_DOF_STAGE)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = _dist()
+    if args.impl == "reference":
+        out = run_reference(args, world, rank, local)
+    else:
+        out = run_ours(args, world, rank, local)
+    if out is not None and rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,127 @@
+/*
+ * opendynamo-b200 — C ABI of the B200 (sm_100a) FR P=3 compressible
+ * Navier–Stokes step path.
+ *
+ * The reference (drunkseal/opendynamo) has no library boundary: its Rust host
+ * NVRTC-compiles four CUDA sources and launches seven kernels by name
+ * (src/solver.rs:432-461, 610-738). This header is the boundary that replaces
+ * that source-level coupling. A host — the bundled C++ runner, the Python
+ * package, or a Rust `solver.rs` through `extern "C"` — owns the step loop's
+ * policy (labels, dumps, checkpoints; src/solver.rs:319-330, 745-818) and
+ * calls these entry points for everything that touches the device.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative OD_ERR_* code; the
+ *    message of the last failure is kept per context (od_last_error). No
+ *    exceptions cross the ABI.
+ *  - State layout is the reference's (src/cuda/rhs.cu:352-361, README
+ *    layout notes): 5 var-major planes rho, rho*u, rho*v, rho*w, E; inside a
+ *    plane element-major blocks of 64 points, point = i + 4 j + 16 k,
+ *    element = ex + nx*ey + nx*ny*ez. Values are of the u_real type.
+ *  - All device work of a context is ordered on its own CUDA stream; calls
+ *    on one context must come from one thread at a time.
+ */
+#ifndef OPENDYNAMO_H
+#define OPENDYNAMO_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OD_FLUX_SLAU2 = 0, OD_FLUX_AUSMPLUS = 1, OD_FLUX_RUSANOV = 2 };
+enum { OD_F32 = 0, OD_F64 = 1 };
+enum {
+    OD_OK = 0,
+    OD_ERR_ARG = -1,    /* invalid argument or unsupported combination */
+    OD_ERR_CUDA = -2,   /* a CUDA call failed (see od_last_error) */
+    OD_ERR_SIZE = -3,   /* buffer size does not match the mesh */
+    OD_ERR_STATE = -4,  /* call out of order (e.g. no state set) */
+    OD_ERR_IO = -5      /* state-file read/write failure */
+};
+
+typedef struct od_ctx od_ctx;
+
+/* Solver parameters. Mirrors the reference's config schema (src/config.rs)
+ * plus the compile-time constants it hardcodes (src/cuda/constants.cuh). */
+typedef struct od_params {
+    int nx, ny, nz;                /* elements per axis ([mesh] nx ny nz) */
+    double lx, ly, lz;             /* box extents; the reference stores them as f32 (config.rs:19-25) */
+    int flux;                      /* OD_FLUX_* ([solver] flux_scheme) */
+    int y_wall;                    /* 1 = slip walls at y = +-ly/2, 0 = periodic ([physics] y_boundary) */
+    int u_real, q_real, rhs_real, compute_real; /* OD_F32 / OD_F64 ([precision] table) */
+    int mixed;                     /* 1 = precision form: f64 state, RK and pressure recovery with
+                                      f32 fluxes; requires u_real = f64, compute_real = f32 */
+    int fast_math;                 /* accepted for config parity ([solver] fast_math) */
+    double mu;                     /* dynamic viscosity; reference constant 1.6e-4 (constants.cuh:42) */
+    double forcing;                /* source added to the rho*u RHS; reference 1e-3 (rhs.cu:508) */
+    int device;                    /* CUDA device ordinal */
+} od_params;
+
+/* Reference defaults: SLAU2, slip walls, all f32, mu 1.6e-4, forcing 1e-3. */
+void od_default_params(od_params* p);
+
+/* Allocate device buffers and prepare the kernels.
+ * Replaces: run_solver_generic setup — compile_module / load_kernels /
+ * setup_fr_operators / allocate_buffers (src/solver.rs:147-159, 432-601). */
+int od_create(const od_params* p, od_ctx** out);
+
+/* Release everything the context owns. */
+void od_destroy(od_ctx* ctx);
+
+/* Bytes of one full state (5 planes of nx*ny*nz*64 u_real values). */
+size_t od_state_bytes(const od_ctx* ctx);
+
+/* Host -> device state upload (blocking).
+ * Replaces: the initial-state upload stream.memcpy_htod (src/solver.rs:197-201). */
+int od_set_state(od_ctx* ctx, const void* host, size_t bytes);
+
+/* Device -> host state download (blocking w.r.t. the context's stream).
+ * Replaces: the dump copy io_stream.memcpy_dtoh (src/solver.rs:757-759). */
+int od_get_state(od_ctx* ctx, void* host, size_t bytes);
+
+/* Same as above from / to device memory (stream-ordered, no host sync). */
+int od_set_state_device(od_ctx* ctx, const void* dptr, size_t bytes);
+int od_get_state_device(od_ctx* ctx, void* dptr, size_t bytes);
+
+/* Enqueue n SSP-RK3 steps of size dt on the context's stream (asynchronous).
+ * Pass dt exactly as the reference does: the configured f32 value widened.
+ * Replaces: the per-step launch sequence launch_rhs_stage + launch_rk_stage
+ * x 3 (src/solver.rs:262-317, 610-738). */
+int od_step(od_ctx* ctx, int n_steps, double dt);
+
+/* Full right-hand side (volume RHS + lifted face corrections) of the current
+ * state into device memory of the u_real type (asynchronous).
+ * Replaces: one launch_rhs_stage followed by the RHS+correction sum of
+ * rk.cu:12-25, exposed for tests and the learned closure. */
+int od_rhs(od_ctx* ctx, void* d_out, size_t bytes);
+
+/* Wait for the context's stream. */
+int od_sync(od_ctx* ctx);
+
+/* The context's cudaStream_t (for events and stream-ordered interop). */
+void* od_stream(od_ctx* ctx);
+
+/* Kernel launches od_step enqueues per step (for launch accounting). */
+int od_launches_per_step(const od_ctx* ctx);
+
+/* Per-kernel timing: when enabled, every stage records CUDA events around its
+ * phase-A and phase-B kernels; od_timing sums the recorded intervals since the
+ * last reset (synchronizes the stream). */
+int od_set_timing(od_ctx* ctx, int enabled);
+int od_timing(od_ctx* ctx, double* ms_phase_a, double* ms_phase_b, long long* n_stages);
+
+/* Message of the last failure on this context ("" if none). */
+const char* od_last_error(const od_ctx* ctx);
+
+/* FR P=3 operator tables in double, as src/fr_math.rs:107-142 builds them:
+ * points[4], D[16] (D[i*4+j] = l'_j(x_i)), extrap_left[4], extrap_right[4],
+ * g_left'[4], g_right'[4]. */
+int od_fr_tables(double* out36);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPENDYNAMO_H */

@@ -1,0 +1,90 @@
+"""ctypes binding of libopendynamo.so (the C ABI in include/opendynamo.h).
+
+The shared library is built in-tree (``python -m opendynamo_b200.build``) and
+there is no fallback: if it is missing, importing a solver raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libopendynamo.so")
+
+OD_FLUX = {"slau2": 0, "ausm+": 1, "rusanov": 2}
+OD_F32, OD_F64 = 0, 1
+
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "size mismatch", -4: "call out of order", -5: "I/O error"}
+
+# every symbol include/opendynamo.h declares
+EXPORTS = (
+    "od_default_params", "od_create", "od_destroy", "od_state_bytes", "od_set_state", "od_get_state",
+    "od_set_state_device", "od_get_state_device", "od_step", "od_rhs", "od_sync", "od_stream",
+    "od_launches_per_step", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
+)
+
+
+class OdParams(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("flux", ctypes.c_int), ("y_wall", ctypes.c_int),
+        ("u_real", ctypes.c_int), ("q_real", ctypes.c_int),
+        ("rhs_real", ctypes.c_int), ("compute_real", ctypes.c_int),
+        ("mixed", ctypes.c_int), ("fast_math", ctypes.c_int),
+        ("mu", ctypes.c_double), ("forcing", ctypes.c_double),
+        ("device", ctypes.c_int),
+    ]
+
+
+class OdError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OdError(f"{LIB_PATH} is missing: build it with `python -m opendynamo_b200.build` "
+                      "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, sz, ci, cd = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double
+    P = ctypes.POINTER(OdParams)
+    sig = {
+        "od_default_params": (None, [P]),
+        "od_create": (ci, [P, ctypes.POINTER(vp)]),
+        "od_destroy": (None, [vp]),
+        "od_state_bytes": (sz, [vp]),
+        "od_set_state": (ci, [vp, vp, sz]),
+        "od_get_state": (ci, [vp, vp, sz]),
+        "od_set_state_device": (ci, [vp, vp, sz]),
+        "od_get_state_device": (ci, [vp, vp, sz]),
+        "od_step": (ci, [vp, ci, cd]),
+        "od_rhs": (ci, [vp, vp, sz]),
+        "od_sync": (ci, [vp]),
+        "od_stream": (vp, [vp]),
+        "od_launches_per_step": (ci, [vp]),
+        "od_set_timing": (ci, [vp, ci]),
+        "od_timing": (ci, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd), ctypes.POINTER(ctypes.c_longlong)]),
+        "od_last_error": (ctypes.c_char_p, [vp]),
+        "od_fr_tables": (ci, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc: int, ctx=None, what: str = "") -> None:
+    if rc != 0:
+        msg = ""
+        if ctx:
+            raw = lib().od_last_error(ctx)
+            msg = raw.decode() if raw else ""
+        raise OdError(f"{what} failed ({ERRORS.get(rc, rc)}): {msg}")

@@ -1,0 +1,428 @@
+// C ABI of the FR P=3 step path (declared in include/opendynamo.h).
+//
+// Owns the device buffers of one solver instance and enqueues the SSP-RK3
+// stages (src/solver.rs:262-317) as phase-A / phase-B kernel pairs on its own
+// stream. The RK scheme needs three state buffers here instead of the
+// reference's two: a phase-A kernel reads its neighbours' state while other
+// blocks write their results, so a stage never writes the buffer it reads.
+//   stage 1: U0 -> U1        u1 = u0 + dt L(u0)
+//   stage 2: U1 (+U0) -> U2  u2 = 3/4 u0 + 1/4 u1 + 1/4 dt L(u1)
+//   stage 3: U2 (+U0) -> U0  u  = 1/3 u0 + 2/3 u2 + 2/3 dt L(u2)
+// Stage 3 overwrites U0 element by element: each thread reads its own
+// point of U0 before writing it, and no other block reads U0 in that stage.
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "../../include/opendynamo.h"
+#include "od_launch.h"
+
+namespace {
+
+// ---- FR operator tables (src/fr_math.rs:3-142), computed on the host in double
+double legendre(int p, double x) {
+    if (p == 0) return 1.0;
+    if (p == 1) return x;
+    double a = 1.0, b = x, val = 0.0;
+    for (int k = 2; k <= p; ++k) {
+        val = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / (double)k;
+        a = b;
+        b = val;
+    }
+    return val;
+}
+
+double dlegendre(int p, double x) {
+    if (p == 0) return 0.0;
+    return (double)p / (x * x - 1.0) * (x * legendre(p, x) - legendre(p - 1, x));
+}
+
+od::TablesD build_tables() {
+    od::TablesD t;
+    const int n = 4, p = 3;
+    for (int i = 0; i < n; ++i) {
+        double x = std::cos(M_PI * (i + 0.75) / (n + 0.5));  // Newton from the Chebyshev-like guess
+        for (int it = 0; it < 100; ++it) {
+            double step = legendre(n, x) / dlegendre(n, x);
+            x -= step;
+            if (std::fabs(step) < 1e-14) break;
+        }
+        t.pts[i] = x;
+    }
+    std::sort(t.pts, t.pts + n);
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) {
+            if (i == j) {
+                double s = 0.0;
+                for (int k = 0; k < n; ++k)
+                    if (k != i) s += 1.0 / (t.pts[i] - t.pts[k]);
+                t.D[i * n + j] = s;
+            } else {
+                double num = 1.0, den = 1.0;
+                for (int k = 0; k < n; ++k) {
+                    if (k != i && k != j) num *= t.pts[i] - t.pts[k];
+                    if (k != j) den *= t.pts[j] - t.pts[k];
+                }
+                t.D[i * n + j] = num / den;
+            }
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        double l = 1.0, r = 1.0;
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            l *= (-1.0 - t.pts[j]) / (t.pts[i] - t.pts[j]);
+            r *= (1.0 - t.pts[j]) / (t.pts[i] - t.pts[j]);
+        }
+        t.eL[i] = l;
+        t.eR[i] = r;
+        double dp = dlegendre(p, t.pts[i]), dp1 = dlegendre(p + 1, t.pts[i]);
+        t.gR[i] = 0.5 * (dp + dp1);
+        t.gL[i] = 0.5 * -1.0 * (dp - dp1);  // (-1)^P with P = 3
+    }
+    return t;
+}
+
+struct Fns {
+    cudaError_t (*launch)(const od::StageLaunch&, cudaStream_t);
+    cudaError_t (*prepare)();
+    bool p_double, c_double, s_double;
+};
+
+Fns combo_fns(od::Combo c) {
+    switch (c) {
+        case od::kF32: return {od::launch_stage_f32, od::prepare_kernels_f32, false, false, false};
+        case od::kF64: return {od::launch_stage_f64, od::prepare_kernels_f64, true, true, true};
+        case od::kU64C32: return {od::launch_stage_u64c32, od::prepare_kernels_u64c32, false, false, true};
+        case od::kU32C64: return {od::launch_stage_u32c64, od::prepare_kernels_u32c64, true, true, false};
+        default: return {od::launch_stage_mixed, od::prepare_kernels_mixed, true, false, true};
+    }
+}
+
+// x evaluated as the given arithmetic type
+double in_type(bool dbl, double x) { return dbl ? x : (double)(float)x; }
+
+}  // namespace
+
+struct od_ctx {
+    od_params p{};
+    od::Combo combo = od::kF32;
+    Fns fns{};
+    cudaStream_t stream = nullptr;
+    void* U[3] = {nullptr, nullptr, nullptr};
+    void* fv = nullptr;
+    size_t state_bytes = 0;
+    size_t elem_size = 4;
+    long long nelem = 0;
+    od::TablesD tab{};
+    double jac[3] = {0, 0, 0};
+    int round_flags = 0;
+    bool have_state = false;
+    int epb_a = 2, epb_b = 4;
+    std::string err;
+    bool timing = false;
+    std::vector<cudaEvent_t> events;
+    size_t ev_used = 0;
+    long long n_stages = 0;
+};
+
+namespace {
+
+int fail(od_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(od_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, OD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int set_device(od_ctx* c) {
+    cudaError_t e = cudaSetDevice(c->p.device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    return OD_OK;
+}
+
+// One stage: phase A (+ phase B) with the given buffers and RK coefficients.
+int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, double ra, double rb, double rc) {
+    od::StageLaunch L{};
+    L.u_in = u_in;
+    L.u0 = u0;
+    L.u_out = u_out;
+    L.fv = c->fv;
+    L.nx = c->p.nx;
+    L.ny = c->p.ny;
+    L.nz = c->p.nz;
+    L.y_wall = c->p.y_wall;
+    L.nelem = c->nelem;
+    L.tab = c->tab;
+    for (int d = 0; d < 3; ++d) L.jac[d] = c->jac[d];
+    L.ra = ra;
+    L.rb = rb;
+    L.rc = rc;
+    L.mu = c->p.mu;
+    L.forcing = c->p.forcing;
+    L.flags = c->round_flags | (u0 ? 1 : 0);
+    L.flux = c->p.flux;
+    L.epb_a = c->epb_a;
+    L.epb_b = c->epb_b;
+    L.phase_b = c->p.mu != 0.0;
+    if (c->timing) {
+        while (c->events.size() < c->ev_used + 3) {
+            cudaEvent_t ev;
+            cudaError_t e = cudaEventCreate(&ev);
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaEventCreate");
+            c->events.push_back(ev);
+        }
+        for (int q = 0; q < 3; ++q) L.ev[q] = c->events[c->ev_used + q];
+        c->ev_used += 3;
+    }
+    cudaError_t e = c->fns.launch(L, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stage launch");
+    c->n_stages++;
+    return OD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void od_default_params(od_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->nx = p->ny = p->nz = 8;
+    p->lx = (double)(4.0f * (float)M_PI);
+    p->ly = 2.0;
+    p->lz = (double)((4.0f / 3.0f) * (float)M_PI);
+    p->flux = OD_FLUX_SLAU2;
+    p->y_wall = 1;
+    p->u_real = p->q_real = p->rhs_real = p->compute_real = OD_F32;
+    p->fast_math = 1;
+    p->mu = 1.6e-4;
+    p->forcing = 1e-3;
+}
+
+int od_fr_tables(double* out) {
+    if (!out) return OD_ERR_ARG;
+    od::TablesD t = build_tables();
+    std::memcpy(out, t.pts, sizeof(t.pts));
+    std::memcpy(out + 4, t.D, sizeof(t.D));
+    std::memcpy(out + 20, t.eL, sizeof(t.eL));
+    std::memcpy(out + 24, t.eR, sizeof(t.eR));
+    std::memcpy(out + 28, t.gL, sizeof(t.gL));
+    std::memcpy(out + 32, t.gR, sizeof(t.gR));
+    return OD_OK;
+}
+
+int od_create(const od_params* p, od_ctx** out) {
+    if (!p || !out) return OD_ERR_ARG;
+    *out = nullptr;
+    if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->flux < 0 || p->flux > 2 || !(p->lx > 0) ||
+        !(p->ly > 0) || !(p->lz > 0))
+        return OD_ERR_ARG;
+    long long nelem = (long long)p->nx * p->ny * p->nz;
+    if (nelem * 64 * 5 >= (1LL << 40)) return OD_ERR_ARG;
+    od_ctx* c = new od_ctx();
+    c->p = *p;
+    c->nelem = nelem;
+    if (p->mixed) {
+        if (p->u_real != OD_F64 || p->compute_real != OD_F32) {
+            delete c;
+            return OD_ERR_ARG;
+        }
+        c->combo = od::kMixed;
+    } else if (p->u_real == OD_F32) {
+        c->combo = p->compute_real == OD_F32 ? od::kF32 : od::kU32C64;
+    } else {
+        c->combo = p->compute_real == OD_F64 ? od::kF64 : od::kU64C32;
+    }
+    c->fns = combo_fns(c->combo);
+    c->elem_size = c->fns.s_double ? 8 : 4;
+    c->state_bytes = (size_t)nelem * 64 * 5 * c->elem_size;
+    // Q / RHS rounding only bites when they are narrower than the compute type
+    if (c->fns.c_double && !p->mixed) {
+        if (p->q_real == OD_F32) c->round_flags |= od::kRoundQ;
+        if (p->rhs_real == OD_F32) c->round_flags |= od::kRoundRhs;
+    }
+    c->tab = build_tables();
+    // jac = 2 / (L / n) in the compute type (rk.cu:93-95)
+    const double L3[3] = {p->lx, p->ly, p->lz};
+    const int n3[3] = {p->nx, p->ny, p->nz};
+    for (int d = 0; d < 3; ++d) {
+        if (c->fns.c_double)
+            c->jac[d] = 2.0 / (L3[d] / (double)n3[d]);
+        else
+            c->jac[d] = (double)(2.0f / ((float)L3[d] / (float)n3[d]));
+    }
+    int rc = set_device(c);
+    if (rc) {
+        *out = c;
+        return rc;
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        *out = c;
+        return cuda_fail(c, e, "cudaStreamCreate");
+    }
+    e = c->fns.prepare();
+    if (e != cudaSuccess) {
+        *out = c;
+        return cuda_fail(c, e, "kernel attributes");
+    }
+    for (int b = 0; b < 3; ++b) {
+        e = cudaMalloc(&c->U[b], c->state_bytes);
+        if (e != cudaSuccess) {
+            *out = c;
+            return cuda_fail(c, e, "cudaMalloc state");
+        }
+    }
+    const size_t fv_bytes = (size_t)nelem * 6 * 4 * 16 * (c->fns.c_double ? 8 : 4);
+    e = cudaMalloc(&c->fv, fv_bytes);
+    if (e != cudaSuccess) {
+        *out = c;
+        return cuda_fail(c, e, "cudaMalloc face buffer");
+    }
+    e = cudaMemsetAsync(c->fv, 0, fv_bytes, c->stream);
+    if (e != cudaSuccess) {
+        *out = c;
+        return cuda_fail(c, e, "cudaMemset");
+    }
+    *out = c;
+    return OD_OK;
+}
+
+void od_destroy(od_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->p.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto ev : c->events) cudaEventDestroy(ev);
+    for (int b = 0; b < 3; ++b)
+        if (c->U[b]) cudaFree(c->U[b]);
+    if (c->fv) cudaFree(c->fv);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+size_t od_state_bytes(const od_ctx* c) { return c ? c->state_bytes : 0; }
+
+int od_set_state(od_ctx* c, const void* host, size_t bytes) {
+    if (!c || !host) return OD_ERR_ARG;
+    if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
+    if (int rc = set_device(c)) return rc;
+    cudaError_t e = cudaMemcpyAsync(c->U[0], host, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "state upload");
+    c->have_state = true;
+    return OD_OK;
+}
+
+int od_get_state(od_ctx* c, void* host, size_t bytes) {
+    if (!c || !host) return OD_ERR_ARG;
+    if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
+    if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    if (int rc = set_device(c)) return rc;
+    cudaError_t e = cudaMemcpyAsync(host, c->U[0], bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "state download");
+    return OD_OK;
+}
+
+int od_set_state_device(od_ctx* c, const void* dptr, size_t bytes) {
+    if (!c || !dptr) return OD_ERR_ARG;
+    if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
+    if (int rc = set_device(c)) return rc;
+    cudaError_t e = cudaMemcpyAsync(c->U[0], dptr, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "state copy");
+    c->have_state = true;
+    return OD_OK;
+}
+
+int od_get_state_device(od_ctx* c, void* dptr, size_t bytes) {
+    if (!c || !dptr) return OD_ERR_ARG;
+    if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
+    if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    if (int rc = set_device(c)) return rc;
+    cudaError_t e = cudaMemcpyAsync(dptr, c->U[0], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "state copy");
+    return OD_OK;
+}
+
+int od_step(od_ctx* c, int n_steps, double dt) {
+    if (!c || n_steps < 0) return OD_ERR_ARG;
+    if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    if (int rc = set_device(c)) return rc;
+    // RK coefficients evaluated in the state-arithmetic type (solver.rs:256, 275-316)
+    const bool pd = c->fns.p_double;
+    const double dtp = in_type(pd, dt);
+    const double c1 = dtp;
+    const double c2 = in_type(pd, in_type(pd, 0.25) * dtp);
+    const double c3 = in_type(pd, in_type(pd, 2.0 / 3.0) * dtp);
+    const double a2 = 0.75, b2 = 0.25;
+    const double a3 = in_type(pd, 1.0 / 3.0), b3 = in_type(pd, 2.0 / 3.0);
+    for (int s = 0; s < n_steps; ++s) {
+        if (int rc = enqueue_stage(c, c->U[0], nullptr, c->U[1], 0.0, 1.0, c1)) return rc;
+        if (int rc = enqueue_stage(c, c->U[1], c->U[0], c->U[2], a2, b2, c2)) return rc;
+        if (int rc = enqueue_stage(c, c->U[2], c->U[0], c->U[0], a3, b3, c3)) return rc;
+    }
+    return OD_OK;
+}
+
+int od_rhs(od_ctx* c, void* d_out, size_t bytes) {
+    if (!c || !d_out) return OD_ERR_ARG;
+    if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "RHS size does not match the mesh");
+    if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    if (d_out == c->U[0]) return fail(c, OD_ERR_ARG, "RHS output must not alias the state");
+    if (int rc = set_device(c)) return rc;
+    return enqueue_stage(c, c->U[0], nullptr, d_out, 0.0, 0.0, 1.0);
+}
+
+int od_sync(od_ctx* c) {
+    if (!c) return OD_ERR_ARG;
+    if (int rc = set_device(c)) return rc;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stream synchronize");
+    return OD_OK;
+}
+
+void* od_stream(od_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int od_launches_per_step(const od_ctx* c) {
+    if (!c) return 0;
+    return 3 * (c->p.mu != 0.0 ? 2 : 1);
+}
+
+int od_set_timing(od_ctx* c, int enabled) {
+    if (!c) return OD_ERR_ARG;
+    if (int rc = od_sync(c)) return rc;
+    c->timing = enabled != 0;
+    c->ev_used = 0;
+    c->n_stages = 0;
+    return OD_OK;
+}
+
+int od_timing(od_ctx* c, double* ms_a, double* ms_b, long long* n_stages) {
+    if (!c) return OD_ERR_ARG;
+    if (int rc = od_sync(c)) return rc;
+    double a = 0, b = 0;
+    for (size_t q = 0; q + 3 <= c->ev_used; q += 3) {
+        float t1 = 0, t2 = 0;
+        cudaError_t e = cudaEventElapsedTime(&t1, c->events[q], c->events[q + 1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t2, c->events[q + 1], c->events[q + 2]);
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaEventElapsedTime");
+        a += t1;
+        b += t2;
+    }
+    if (ms_a) *ms_a = a;
+    if (ms_b) *ms_b = b;
+    if (n_stages) *n_stages = (long long)(c->ev_used / 3);
+    c->ev_used = 0;
+    return OD_OK;
+}
+
+const char* od_last_error(const od_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// Host-side launch interface between the C-ABI layer and the templated
+// stage kernels. Each precision combination is compiled in its own
+// translation unit (od_inst_*.cu) so the kernel variants build in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace od {
+
+enum StageFlags : int {
+    kHasU0 = 1,      // out = ra*u0 + rb*u_in + rc*R (else rb*u_in + rc*R)
+    kRoundQ = 2,     // round the gradient through f32 (q_real = f32 with f64 compute)
+    kRoundRhs = 4,   // round the volume RHS through f32 (rhs_real = f32 with f64 compute)
+};
+
+// FR operator tables in double (the host computes them once, as
+// src/fr_math.rs:107-142 does, then each launch casts to its own types).
+struct TablesD {
+    double pts[4], D[16], eL[4], eR[4], gL[4], gR[4];
+};
+
+struct StageLaunch {
+    const void* u_in;
+    const void* u0;      // null on stage 1 / single RHS evaluations
+    void* u_out;
+    void* fv;            // viscous face buffer
+    int nx, ny, nz, y_wall;
+    long long nelem;
+    TablesD tab;
+    double jac[3];       // already evaluated in the compute type
+    double ra, rb, rc;   // already evaluated in the state-arithmetic type
+    double mu, forcing;
+    int flags;           // kHasU0 | kRoundQ | kRoundRhs
+    int flux;            // 0 slau2, 1 ausm+, 2 rusanov
+    int epb_a, epb_b;    // elements per block of phase A / phase B
+    bool phase_b;        // launch phase B (viscous neighbour term)
+    cudaEvent_t ev[3];   // optional timing events: before A, between A and B, after B
+};
+
+// Precision combination ids: stored type / state arithmetic / flux arithmetic
+enum Combo : int {
+    kF32 = 0,      // float / float / float
+    kF64 = 1,      // double / double / double
+    kU64C32 = 2,   // double / float / float   (reference pipeline with u_real = f64, compute_real = f32)
+    kU32C64 = 3,   // float / double / double
+    kMixed = 4,    // double / double / float  (precision form: f64 state, RK and pressure; f32 fluxes)
+};
+
+cudaError_t launch_stage_f32(const StageLaunch& L, cudaStream_t s);
+cudaError_t launch_stage_f64(const StageLaunch& L, cudaStream_t s);
+cudaError_t launch_stage_u64c32(const StageLaunch& L, cudaStream_t s);
+cudaError_t launch_stage_u32c64(const StageLaunch& L, cudaStream_t s);
+cudaError_t launch_stage_mixed(const StageLaunch& L, cudaStream_t s);
+
+// Set the dynamic shared-memory limits of every kernel variant once per device.
+cudaError_t prepare_kernels_f32();
+cudaError_t prepare_kernels_f64();
+cudaError_t prepare_kernels_u64c32();
+cudaError_t prepare_kernels_u32c64();
+cudaError_t prepare_kernels_mixed();
+
+}  // namespace od

@@ -1,0 +1,127 @@
+// Templated host launcher for one precision combination; included by the
+// od_inst_*.cu translation units only.
+#pragma once
+
+#include "od_launch.h"
+#include "od_stage.cuh"
+
+namespace od {
+
+template <class T>
+Tab<T> cast_tab(const TablesD& t) {
+    Tab<T> r;
+    for (int i = 0; i < 16; ++i) r.D[i] = (T)t.D[i];
+    for (int i = 0; i < 4; ++i) {
+        r.eL[i] = (T)t.eL[i];
+        r.eR[i] = (T)t.eR[i];
+        r.gL[i] = (T)t.gL[i];
+        r.gR[i] = (T)t.gR[i];
+    }
+    return r;
+}
+
+template <class S, class P, class C, int FLUX, int EPB>
+cudaError_t launch_a(const StageAParams<S, P, C>& A, long long nelem, cudaStream_t s) {
+    const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
+    const size_t smem = sizeof(SlotA<P, C>) * EPB;
+    stage_a_kernel<S, P, C, FLUX, EPB><<<grid, 64 * EPB, smem, s>>>(A);
+    return cudaGetLastError();
+}
+
+template <class S, class P, class C, int FLUX>
+cudaError_t launch_a_epb(const StageAParams<S, P, C>& A, long long nelem, int epb, cudaStream_t s) {
+    switch (epb) {
+        case 1: return launch_a<S, P, C, FLUX, 1>(A, nelem, s);
+        case 4: return launch_a<S, P, C, FLUX, 4>(A, nelem, s);
+        default: return launch_a<S, P, C, FLUX, 2>(A, nelem, s);
+    }
+}
+
+template <class S, class P, class C, int EPB>
+cudaError_t launch_b(const StageBParams<S, P, C>& B, long long nelem, cudaStream_t s) {
+    const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
+    stage_b_kernel<S, P, C, EPB><<<grid, 64 * EPB, 0, s>>>(B);
+    return cudaGetLastError();
+}
+
+template <class S, class P, class C>
+cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
+    StageAParams<S, P, C> A;
+    A.u_in = (const S*)L.u_in;
+    A.u0 = (const S*)L.u0;
+    A.u_out = (S*)L.u_out;
+    A.fv = (C*)L.fv;
+    A.m.nx = L.nx;
+    A.m.ny = L.ny;
+    A.m.nz = L.nz;
+    A.m.y_wall = L.y_wall;
+    A.m.nelem = L.nelem;
+    A.m.npts = L.nelem * NE;
+    A.tp = cast_tab<P>(L.tab);
+    A.tc = cast_tab<C>(L.tab);
+    for (int d = 0; d < 3; ++d) A.jac[d] = (C)L.jac[d];
+    A.ra = (P)L.ra;
+    A.rb = (P)L.rb;
+    A.rc = (P)L.rc;
+    A.mu = (C)L.mu;
+    A.forcing = (C)L.forcing;
+    A.flags = L.flags;
+    if (L.ev[0]) cudaEventRecord(L.ev[0], s);
+    cudaError_t err;
+    switch (L.flux) {
+        case kSlau2: err = launch_a_epb<S, P, C, kSlau2>(A, L.nelem, L.epb_a, s); break;
+        case kAusmPlus: err = launch_a_epb<S, P, C, kAusmPlus>(A, L.nelem, L.epb_a, s); break;
+        default: err = launch_a_epb<S, P, C, kRusanov>(A, L.nelem, L.epb_a, s); break;
+    }
+    if (err != cudaSuccess) return err;
+    if (L.ev[1]) cudaEventRecord(L.ev[1], s);
+    if (L.phase_b) {
+        StageBParams<S, P, C> B;
+        B.u_out = (S*)L.u_out;
+        B.fv = (const C*)L.fv;
+        B.m = A.m;
+        B.tc = A.tc;
+        for (int d = 0; d < 3; ++d) B.jac[d] = A.jac[d];
+        B.rc = A.rc;
+        switch (L.epb_b) {
+            case 2: err = launch_b<S, P, C, 2>(B, L.nelem, s); break;
+            case 8: err = launch_b<S, P, C, 8>(B, L.nelem, s); break;
+            default: err = launch_b<S, P, C, 4>(B, L.nelem, s); break;
+        }
+        if (err != cudaSuccess) return err;
+    }
+    if (L.ev[2]) cudaEventRecord(L.ev[2], s);
+    return cudaSuccess;
+}
+
+template <class S, class P, class C, int FLUX>
+cudaError_t prepare_flux() {
+    cudaError_t e;
+    e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(SlotA<P, C>) * 1));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(SlotA<P, C>) * 2));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(SlotA<P, C>) * 4));
+}
+
+template <class S, class P, class C>
+cudaError_t prepare_t() {
+    cudaError_t e = prepare_flux<S, P, C, kSlau2>();
+    if (e != cudaSuccess) return e;
+    e = prepare_flux<S, P, C, kAusmPlus>();
+    if (e != cudaSuccess) return e;
+    return prepare_flux<S, P, C, kRusanov>();
+}
+
+}  // namespace od
+
+#define OD_INSTANTIATE(NAME, S, P, C)                                                          \
+    namespace od {                                                                             \
+    cudaError_t launch_stage_##NAME(const StageLaunch& L, cudaStream_t s) {                   \
+        return launch_stage_t<S, P, C>(L, s);                                                  \
+    }                                                                                          \
+    cudaError_t prepare_kernels_##NAME() { return prepare_t<S, P, C>(); }                      \
+    }
