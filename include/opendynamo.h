@@ -106,6 +106,11 @@ void* od_stream(od_ctx* ctx);
 /* Kernel launches od_step enqueues per step (for launch accounting). */
 int od_launches_per_step(const od_ctx* ctx);
 
+/* Launch shape: elements per thread block of the phase-A kernel (2, 4 or 8;
+ * 16 threads per element) and of the phase-B kernel (8 or 16). Results do
+ * not depend on it; the autotuner picks it per mesh and precision. */
+int od_set_launch_shape(od_ctx* ctx, int elems_per_block_a, int elems_per_block_b);
+
 /* Per-kernel timing: when enabled, every stage records CUDA events around its
  * phase-A and phase-B kernels; od_timing sums the recorded intervals since the
  * last reset (synchronizes the stream). */

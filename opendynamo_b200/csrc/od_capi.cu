@@ -122,7 +122,7 @@ struct od_ctx {
     double jac[3] = {0, 0, 0};
     int round_flags = 0;
     bool have_state = false;
-    int epb_a = 2, epb_b = 4;
+    int epb_a = 4, epb_b = 16;
     std::string err;
     bool timing = false;
     std::vector<cudaEvent_t> events;
@@ -393,6 +393,17 @@ void* od_stream(od_ctx* c) { return c ? (void*)c->stream : nullptr; }
 int od_launches_per_step(const od_ctx* c) {
     if (!c) return 0;
     return 3 * (c->p.mu != 0.0 ? 2 : 1);
+}
+
+int od_set_launch_shape(od_ctx* c, int elems_per_block_a, int elems_per_block_b) {
+    if (!c) return OD_ERR_ARG;
+    if (elems_per_block_a != 2 && elems_per_block_a != 4 && elems_per_block_a != 8)
+        return fail(c, OD_ERR_ARG, "phase-A elements per block must be 2, 4 or 8");
+    if (elems_per_block_b != 8 && elems_per_block_b != 16)
+        return fail(c, OD_ERR_ARG, "phase-B elements per block must be 8 or 16");
+    c->epb_a = elems_per_block_a;
+    c->epb_b = elems_per_block_b;
+    return OD_OK;
 }
 
 int od_set_timing(od_ctx* c, int enabled) {

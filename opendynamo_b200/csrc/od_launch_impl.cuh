@@ -24,23 +24,23 @@ template <class S, class P, class C, int FLUX, int EPB>
 cudaError_t launch_a(const StageAParams<S, P, C>& A, long long nelem, cudaStream_t s) {
     const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
     const size_t smem = sizeof(SlotA<P, C>) * EPB;
-    stage_a_kernel<S, P, C, FLUX, EPB><<<grid, 64 * EPB, smem, s>>>(A);
+    stage_a_kernel<S, P, C, FLUX, EPB><<<grid, LPE * EPB, smem, s>>>(A);
     return cudaGetLastError();
 }
 
 template <class S, class P, class C, int FLUX>
 cudaError_t launch_a_epb(const StageAParams<S, P, C>& A, long long nelem, int epb, cudaStream_t s) {
     switch (epb) {
-        case 1: return launch_a<S, P, C, FLUX, 1>(A, nelem, s);
-        case 4: return launch_a<S, P, C, FLUX, 4>(A, nelem, s);
-        default: return launch_a<S, P, C, FLUX, 2>(A, nelem, s);
+        case 2: return launch_a<S, P, C, FLUX, 2>(A, nelem, s);
+        case 8: return launch_a<S, P, C, FLUX, 8>(A, nelem, s);
+        default: return launch_a<S, P, C, FLUX, 4>(A, nelem, s);
     }
 }
 
 template <class S, class P, class C, int EPB>
 cudaError_t launch_b(const StageBParams<S, P, C>& B, long long nelem, cudaStream_t s) {
     const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
-    stage_b_kernel<S, P, C, EPB><<<grid, 64 * EPB, 0, s>>>(B);
+    stage_b_kernel<S, P, C, EPB><<<grid, LPE * EPB, 0, s>>>(B);
     return cudaGetLastError();
 }
 
@@ -84,9 +84,8 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
         for (int d = 0; d < 3; ++d) B.jac[d] = A.jac[d];
         B.rc = A.rc;
         switch (L.epb_b) {
-            case 2: err = launch_b<S, P, C, 2>(B, L.nelem, s); break;
             case 8: err = launch_b<S, P, C, 8>(B, L.nelem, s); break;
-            default: err = launch_b<S, P, C, 4>(B, L.nelem, s); break;
+            default: err = launch_b<S, P, C, 16>(B, L.nelem, s); break;
         }
         if (err != cudaSuccess) return err;
     }
@@ -97,14 +96,14 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
 template <class S, class P, class C, int FLUX>
 cudaError_t prepare_flux() {
     cudaError_t e;
-    e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(SlotA<P, C>) * 1));
-    if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(SlotA<P, C>) * 2));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(SlotA<P, C>) * 4));
+    e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(SlotA<P, C>) * 4));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(SlotA<P, C>) * 8));
 }
 
 template <class S, class P, class C>

@@ -1,31 +1,34 @@
 // FR P=3 stage kernels for sm_100a.
 //
-// One SSP-RK3 stage of the reference (src/solver.rs:262-317) is the
-// volume kernel, three face kernels (+ the y-wall kernel) and the RK kernel
+// One SSP-RK3 stage of the reference (src/solver.rs:262-317) is a volume
+// kernel, three face kernels (+ the y-wall kernel) and an RK kernel
 // (src/cuda/rhs.cu:344-739, src/cuda/rk.cu:85-115): seven passes over HBM
-// with 6 gradient slice arrays and 6 face-correction arrays in between.
-// Here a stage is two element-local phases:
+// with 6 gradient-slice and 6 face-correction arrays in between. Here a
+// stage is two element-local kernels.
 //
-//  phase A (one element per 64 threads)
-//    - stage the element's 5x64 state in shared memory,
-//    - face values of the element and of its six neighbours (BR1 common
-//      solution, slip-wall mirror of rhs.cu:111-114),
-//    - corrected gradient (rhs.cu:373-455) kept in registers + shared memory,
-//    - volume divergence of F_euler - F_viscous (rhs.cu:229-266),
-//    - at all 6 faces: the interface flux F_I from the two face states, the
-//      element's own Euler and viscous face fluxes; the element's face
-//      correction j = F_I - 1/2 (Fv_own + Fv_nbr) - (Fe_own - Fv_own)
-//      (rhs.cu:273-297) is formed up to its -1/2 Fv_nbr term,
-//    - correction lifting with the Radau g' (rk.cu:12-25) and the RK
-//      combination a*u0 + b*u + c*(RHS + lift) (rk.cu:27-83),
-//    - the element's own viscous face flux (4 non-zero components) is
-//      written to a small face buffer for its neighbours;
-//  phase B (one element per 64 threads)
-//    - adds c * lift(-1/2 Fv_nbr) for the element's non-wall faces.
-//
-// Only the viscous flux needs the neighbour's *gradient*, which depends on
-// the neighbour's neighbours; splitting it out is what lets everything else
-// run in one pass. Phase B is skipped when mu == 0.
+// Phase A — 16 threads per element; in the pass of direction d each thread
+// owns the d-line through face point l (l = j+4k for x, i+4k for y, i+4j for
+// z, the reference's face-point numbering), so 1-D operators act on four
+// registers:
+//   P1  the element state (x-lines, 128-bit loads) -> registers + smem
+//   P2-4 per direction: own and neighbour face values (BR1 common solution,
+//        slip-wall mirror rhs.cu:111-114), corrected gradient along the line
+//        (rhs.cu:373-461), interface flux F_I and own Euler flux at the two
+//        faces of the line -> j = F_I - Fe_own (slip wall: [0,0,p_w,0,0] - Fe)
+//   P5-6 y / z faces: gradient at the face (11 components), own viscous
+//        flux Fv; j += 1/2 Fv_own; Fv_own -> face buffer for the neighbour
+//   P7  x-threads: pointwise Euler - viscous fluxes of their 4 points
+//        (rhs.cu:229-266), x-divergence in registers, x-face viscous flux
+//   P8-9 y / z divergence along the lines
+//   P10 x-threads: RHS = -div + forcing (rhs.cu:505-509), lifting
+//        -(j_L g_L' + j_R g_R') jac (rk.cu:12-25), RK combination
+//        a*u0 + b*u + c*(RHS + lift) (rk.cu:27-83), 128-bit stores.
+//   The face correction of the reference, j = F_I - 1/2(Fv_L + Fv_R) -
+//   (Fe_own - Fv_own), is complete here except for -1/2 Fv_nbr.
+// Phase B — adds c * lift(-1/2 Fv_nbr) over the element's non-wall faces.
+// Only the neighbour's viscous face flux depends on the neighbour's
+// gradient (hence on its own neighbours); everything else is element-local
+// given the six neighbours' face values. Phase B is skipped when mu == 0.
 //
 // Types: S = stored state, P = state arithmetic (face values, pressure
 // recovery, RK accumulation), C = flux arithmetic. Reference-compatible
@@ -42,6 +45,7 @@ constexpr int NP = 4;   // points per direction
 constexpr int NF = 16;  // points per face
 constexpr int NE = 64;  // points per element
 constexpr int NV = 5;   // conserved variables
+constexpr int LPE = 16; // threads (lines) per element
 
 template <class T>
 struct Tab {
@@ -58,70 +62,112 @@ struct Mesh {
 };
 
 // point index inside an element: i + 4 j + 16 k
-__device__ __forceinline__ int pid(int i, int j, int k) { return i + NP * j + NF * k; }
+__device__ __forceinline__ constexpr int pid(int i, int j, int k) { return i + NP * j + NF * k; }
 
-// point m of the direction-d line through face point fp
-// (fp = j + 4k for x, i + 4k for y, i + 4j for z, as the reference's faces)
-__device__ __forceinline__ int line_pt(int d, int fp, int m) {
-    const int a = fp & 3, b = fp >> 2;
-    return d == 0 ? pid(m, a, b) : (d == 1 ? pid(a, m, b) : pid(a, b, m));
+// point m of the direction-D line through face point fp
+template <int D>
+__device__ __forceinline__ int line_pt(int fp, int m) {
+    if constexpr (D == 0) return m + NP * fp;                  // fp = j + 4k
+    else if constexpr (D == 1) return (fp & 3) + NP * m + NF * (fp >> 2);  // fp = i + 4k
+    else return fp + NF * m;                                   // fp = i + 4j
 }
 
 // Face value from the four samples of a line; one fixed FMA chain so that the
 // two elements sharing a face compute bit-identical face states.
 template <class T>
-__device__ __forceinline__ T trace4(T q0, T q1, T q2, T q3, const T* c) {
-    return fma(q3, c[3], fma(q2, c[2], fma(q1, c[1], q0 * c[0])));
+__device__ __forceinline__ T trace4(const T* q, const T* c) {
+    return fma(q[3], c[3], fma(q[2], c[2], fma(q[1], c[1], q[0] * c[0])));
 }
 
 // neighbour across face (d, side) or -1 for a slip wall
 __device__ __forceinline__ long long neighbour(const Mesh& m, int ex, int ey, int ez, int d, int side) {
-    int c[3] = {ex, ey, ez};
-    const int n[3] = {m.nx, m.ny, m.nz};
-    int tgt = c[d] + (side ? 1 : -1);
-    if (d == 1 && m.y_wall && (tgt < 0 || tgt >= n[1])) return -1;
-    if (tgt < 0) tgt += n[d];
-    if (tgt >= n[d]) tgt -= n[d];
-    c[d] = tgt;
-    return (long long)c[0] + (long long)m.nx * ((long long)c[1] + (long long)m.ny * c[2]);
+    int c0 = ex, c1 = ey, c2 = ez;
+    if (d == 0) {
+        c0 += side ? 1 : -1;
+        c0 = c0 < 0 ? c0 + m.nx : (c0 >= m.nx ? c0 - m.nx : c0);
+    } else if (d == 1) {
+        c1 += side ? 1 : -1;
+        if (m.y_wall && (c1 < 0 || c1 >= m.ny)) return -1;
+        c1 = c1 < 0 ? c1 + m.ny : (c1 >= m.ny ? c1 - m.ny : c1);
+    } else {
+        c2 += side ? 1 : -1;
+        c2 = c2 < 0 ? c2 + m.nz : (c2 >= m.nz ? c2 - m.nz : c2);
+    }
+    return (long long)c0 + (long long)m.nx * ((long long)c1 + (long long)m.ny * c2);
 }
 
-// Load the 4 samples of a neighbour's line from global memory.
-template <class S, class P>
-__device__ __forceinline__ void load_line(const S* __restrict__ base, int d, int fp, P* q) {
-    if (d == 0) {
-        const S* p = base + 4 * fp;
-        if constexpr (sizeof(S) == 4) {
-            float4 v = __ldg(reinterpret_cast<const float4*>(p));
-            q[0] = (P)v.x; q[1] = (P)v.y; q[2] = (P)v.z; q[3] = (P)v.w;
-        } else {
-            double2 a = __ldg(reinterpret_cast<const double2*>(p));
-            double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-            q[0] = (P)a.x; q[1] = (P)a.y; q[2] = (P)b.x; q[3] = (P)b.y;
-        }
+// ---- 4-wide loads / stores (16-byte aligned for float, 32-byte for double)
+template <class T>
+__device__ __forceinline__ void ld4s(const T* p, T* q) {
+    if constexpr (sizeof(T) == 4) {
+        float4 v = *reinterpret_cast<const float4*>(p);
+        q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = v.w;
     } else {
-#pragma unroll
-        for (int mm = 0; mm < 4; ++mm) q[mm] = (P)__ldg(base + line_pt(d, fp, mm));
+        double2 a = reinterpret_cast<const double2*>(p)[0];
+        double2 b = reinterpret_cast<const double2*>(p)[1];
+        q[0] = a.x; q[1] = a.y; q[2] = b.x; q[3] = b.y;
     }
 }
 
-// which gradient components the direction-d viscous flux reads
-__device__ __forceinline__ bool grad_used(int d, int c) {
-    // x omits 8,10,13,14; y omits 5,9,12,14; z omits 4,6,12,13 (rhs.cu:129,151,169)
-    const unsigned omit = d == 0 ? ((1u << 8) | (1u << 10) | (1u << 13) | (1u << 14))
-                        : d == 1 ? ((1u << 5) | (1u << 9) | (1u << 12) | (1u << 14))
-                                 : ((1u << 4) | (1u << 6) | (1u << 12) | (1u << 13));
+template <class T>
+__device__ __forceinline__ void st4s(T* p, const T* q) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(q[0], q[1], q[2], q[3]);
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2(q[0], q[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(q[2], q[3]);
+    }
+}
+
+// global 4-wide load of S values converted to P (read-only path)
+template <class S, class P>
+__device__ __forceinline__ void ldg4(const S* __restrict__ p, P* q) {
+    if constexpr (sizeof(S) == 4) {
+        float4 v = __ldg(reinterpret_cast<const float4*>(p));
+        q[0] = (P)v.x; q[1] = (P)v.y; q[2] = (P)v.z; q[3] = (P)v.w;
+    } else {
+        double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        q[0] = (P)a.x; q[1] = (P)a.y; q[2] = (P)b.x; q[3] = (P)b.y;
+    }
+}
+
+// coherent 4-wide load (for data the same kernel later overwrites)
+template <class S, class P>
+__device__ __forceinline__ void ldc4(const S* p, P* q) {
+    S w[4];
+    ld4s(p, w);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) q[a] = (P)w[a];
+}
+
+template <class S, class P>
+__device__ __forceinline__ void stg4(S* p, const P* q) {
+    if constexpr (sizeof(S) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2((double)q[0], (double)q[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2((double)q[2], (double)q[3]);
+    }
+}
+
+// gradient components the direction-D viscous flux reads
+// (x omits 8,10,13,14; y omits 5,9,12,14; z omits 4,6,12,13 — rhs.cu:129,151,169)
+template <int D>
+__device__ __forceinline__ constexpr bool grad_used(int c) {
+    constexpr unsigned omit = D == 0 ? ((1u << 8) | (1u << 10) | (1u << 13) | (1u << 14))
+                            : D == 1 ? ((1u << 5) | (1u << 9) | (1u << 12) | (1u << 14))
+                                     : ((1u << 4) | (1u << 6) | (1u << 12) | (1u << 13));
     return !((omit >> c) & 1u);
 }
 
 // Shared-memory slot of one element in phase A.
 template <class P, class C>
-struct SlotA {
-    P u[NV][NE];            // element state
-    P tr[3][2][NV][NF];     // own face values  [dir][side][var][face pt]
-    P nb[3][2][NV][NF];     // neighbour face values
-    C g[15][NE];            // corrected gradient; reused for the volume fluxes F[3][5][64]
-    C j[3][2][NV][NF];      // face corrections without the -1/2 Fv_nbr part
+struct alignas(16) SlotA {
+    C g[15][NE];          // gradient; after P7 F_y in rows 0-4, F_z in 5-9; after P8 div_y in 10-14
+    P u[NV][NE];          // state; after P9 div_z (as C)
+    P tr[6][NV][NF];      // own face values [face = 2d + side][var][face pt]
+    C j[6][NV][NF];       // face corrections without -1/2 Fv_nbr
 };
 
 template <class S, class P, class C>
@@ -139,62 +185,188 @@ struct StageAParams {
     int flags;
 };
 
-// One face point of phase A, direction D.
+// Interface-flux part of the face correction at one face point, side `side`
+// of direction D: j = F_I - Fe_own, or the slip-wall flux minus Fe_own.
+template <int FLUX, int D, class P, class C>
+__device__ __forceinline__ void inviscid_face(const P* own, const P* nbr, int side, bool wall, C* j) {
+    FaceState<C> so = make_face_state<C, P>(own);
+    C fe[NV];
+    euler_flux<D>(so, fe);
+    if (wall) {
+        // F_wall = [0, 0, p_wall, 0, 0], p_wall from the own flux (rhs.cu:321-326)
+        const C pw = fe[2] - so.q[2] * so.q[2] * so.ir;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) j[v] = -fe[v];
+        j[2] = pw - fe[2];
+        return;
+    }
+    FaceState<C> sn = make_face_state<C, P>(nbr);
+    C fi[NV];
+    if (side)
+        interface_flux<FLUX, D>(so, sn, fi);
+    else
+        interface_flux<FLUX, D>(sn, so, fi);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) j[v] = fi[v] - fe[v];
+}
+
+// P2-P4: one direction of the gradient / face-value pass for line l.
 template <int FLUX, int D, class S, class P, class C>
-__device__ __forceinline__ void face_point(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int side,
-                                           int fp, bool wall) {
-    P qo[NV], qn[NV];
+__device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, int l,
+                                          const long long nb0, const long long nb1, const P (*qreg)[4]) {
+    const Mesh& m = A.m;
+    P q[NV][4];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        qo[v] = sm.tr[D][side][v][fp];
-        qn[v] = sm.nb[D][side][v][fp];
+        if constexpr (D == 0) {
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) q[v][mm] = qreg[v][mm];
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) q[v][mm] = sm.u[v][line_pt<D>(l, mm)];
+        }
     }
-    // own gradient at the face (the 11 components the D-flux reads)
-    C gt[15];
-    const C* ec = side ? A.tc.eR : A.tc.eL;
+    P oL[NV], oR[NV], nL[NV], nR[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        oL[v] = trace4(q[v], A.tp.eL);
+        oR[v] = trace4(q[v], A.tp.eR);
+        const P refl = (v > 0 && v < 4) ? (P)-1.0 : (P)1.0;
+        if (nb0 >= 0) {
+            P w[4];
+            const S* base = A.u_in + v * m.npts + nb0 * NE;
+            if constexpr (D == 0) {
+                ldg4<S, P>(base + 4 * l, w);
+            } else {
+#pragma unroll
+                for (int mm = 0; mm < 4; ++mm) w[mm] = (P)__ldg(base + line_pt<D>(l, mm));
+            }
+            nL[v] = trace4(w, A.tp.eR);
+        } else {
+            nL[v] = oL[v] * refl;
+        }
+        if (nb1 >= 0) {
+            P w[4];
+            const S* base = A.u_in + v * m.npts + nb1 * NE;
+            if constexpr (D == 0) {
+                ldg4<S, P>(base + 4 * l, w);
+            } else {
+#pragma unroll
+                for (int mm = 0; mm < 4; ++mm) w[mm] = (P)__ldg(base + line_pt<D>(l, mm));
+            }
+            nR[v] = trace4(w, A.tp.eL);
+        } else {
+            nR[v] = oR[v] * refl;
+        }
+    }
+    // corrected gradient along the line (BR1)
+    const C jac = A.jac[D];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const C jl = (C)((P)0.5 * (nL[v] + oL[v]) - oL[v]);
+        const C jr = (C)((P)0.5 * (nR[v] + oR[v]) - oR[v]);
+        C qc[4] = {(C)q[v][0], (C)q[v][1], (C)q[v][2], (C)q[v][3]};
+        C gv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            C der = (C)0;
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) der = fma(A.tc.D[a * 4 + mm], qc[mm], der);
+            C gg = der * jac;
+            gg += jl * A.tc.gL[a] * jac;
+            gg += jr * A.tc.gR[a] * jac;
+            if constexpr (sizeof(C) == 8) {
+                if (A.flags & kRoundQ) gg = (C)(float)gg;
+            }
+            gv[a] = gg;
+        }
+        if constexpr (D == 0) {
+            st4s(&sm.g[3 * v][4 * l], gv);
+        } else {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) sm.g[3 * v + D][line_pt<D>(l, a)] = gv[a];
+        }
+        sm.tr[2 * D][v][l] = oL[v];
+        sm.tr[2 * D + 1][v][l] = oR[v];
+    }
+    // interface fluxes at the two faces of this line
+    C j0[NV], j1[NV];
+    inviscid_face<FLUX, D, P, C>(oL, nL, 0, nb0 < 0, j0);
+    inviscid_face<FLUX, D, P, C>(oR, nR, 1, nb1 < 0, j1);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        sm.j[2 * D][v][l] = j0[v];
+        sm.j[2 * D + 1][v][l] = j1[v];
+    }
+}
+
+// Viscous part at one face point: j += 1/2 Fv_own; Fv_own (components 1..4)
+// to the face buffer for the neighbour's phase B.
+template <int D, class S, class P, class C>
+__device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
+                                             int side, const C* gt, bool live) {
+    const int f = 2 * D + side;
+    P qp[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qp[v] = sm.tr[f][v][l];
+    FaceState<C> s = make_face_state<C, P>(qp);
+    const C praw = (C)raw_pressure<P>(qp[0], qp[1], qp[2], qp[3], qp[4]);
+    C fv[NV];
+    viscous_flux<D>(s, praw, gt, A.mu, fv);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sm.j[f][v][l] += (C)0.5 * fv[v];
+    if (live) {
+        C* out = A.fv + ((e * 6 + f) * 4) * NF + l;
+#pragma unroll
+        for (int v = 1; v < NV; ++v) out[(v - 1) * NF] = fv[v];
+    }
+}
+
+// P5 / P6: face gradient along the y or z line of thread l, both faces.
+template <int D, class S, class P, class C>
+__device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
+                                               bool wall0, bool wall1, bool live) {
+    C gL[15], gR[15];
 #pragma unroll
     for (int c = 0; c < 15; ++c) {
-        if (!grad_used(D, c)) {
-            gt[c] = (C)0;
+        if (!grad_used<D>(c)) {
+            gL[c] = (C)0;
+            gR[c] = (C)0;
             continue;
         }
-        gt[c] = trace4(sm.g[c][line_pt(D, fp, 0)], sm.g[c][line_pt(D, fp, 1)], sm.g[c][line_pt(D, fp, 2)],
-                       sm.g[c][line_pt(D, fp, 3)], ec);
+        C w[4];
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) w[mm] = sm.g[c][line_pt<D>(l, mm)];
+        gL[c] = trace4(w, A.tc.eL);
+        gR[c] = trace4(w, A.tc.eR);
     }
-    FaceState<C> so = make_face_state<C, P>(qo);
-    C praw_o = (C)raw_pressure<P>(qo[0], qo[1], qo[2], qo[3], qo[4]);
-    C fvo[NV], feo[NV], jv[NV];
-    viscous_flux<D>(so, praw_o, gt, A.mu, fvo);
-    euler_flux<D>(so, feo);
-    if (wall) {
-        // slip wall: F = [0, 0, p_wall, 0, 0] with p_wall from the own flux
-        // (rhs.cu:311-339); the viscous traction cancels exactly.
-        C fw2 = feo[2] - so.q[2] * so.q[2] * so.ir;
+    if (!wall0) viscous_face<D>(A, sm, e, l, 0, gL, live);
+    if (!wall1) viscous_face<D>(A, sm, e, l, 1, gR, live);
+}
+
+// P8 / P9: divergence of F_D along the line of thread l.
+template <int D, class C>
+__device__ __forceinline__ void div_pass(const C (*F)[NE], C* out, int l, const C* Dm, C jac) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) jv[v] = -feo[v];
-        jv[2] = fw2 - feo[2];
-    } else {
-        FaceState<C> sn = make_face_state<C, P>(qn);
-        C fi[NV];
-        if (side)
-            interface_flux<FLUX, D>(so, sn, fi);
-        else
-            interface_flux<FLUX, D>(sn, so, fi);
+    for (int v = 0; v < NV; ++v) {
+        C w[4];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) jv[v] = fi[v] - feo[v] + (C)0.5 * fvo[v];
-        C* out = A.fv + ((e * 6 + 2 * D + side) * 4) * NF + fp;
+        for (int mm = 0; mm < 4; ++mm) w[mm] = F[v][line_pt<D>(l, mm)];
 #pragma unroll
-        for (int v = 1; v < NV; ++v) out[(v - 1) * NF] = fvo[v];
+        for (int a = 0; a < 4; ++a) {
+            C df = (C)0;
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) df = fma(Dm[a * 4 + mm], w[mm], df);
+            out[v * NE + line_pt<D>(l, a)] = df * jac;
+        }
     }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) sm.j[D][side][v][fp] = jv[v];
 }
 
 template <class S, class P, class C, int FLUX, int EPB>
-__global__ void __launch_bounds__(64 * EPB) stage_a_kernel(const StageAParams<S, P, C> A) {
+__global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S, P, C> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int t = threadIdx.x & 63;
-    const int es = threadIdx.x >> 6;
+    const int l = threadIdx.x & (LPE - 1);
+    const int es = threadIdx.x / LPE;
     SlotA<P, C>& sm = reinterpret_cast<SlotA<P, C>*>(smem_raw)[es];
     const long long e = (long long)blockIdx.x * EPB + es;
     const bool live = e < A.m.nelem;
@@ -203,159 +375,116 @@ __global__ void __launch_bounds__(64 * EPB) stage_a_kernel(const StageAParams<S,
     const int ex = (int)(ec % m.nx);
     const int ey = (int)((ec / m.nx) % m.ny);
     const int ez = (int)(ec / ((long long)m.nx * m.ny));
-    const int ia[3] = {t & 3, (t >> 2) & 3, t >> 4};               // position along x, y, z
-    const int fpa[3] = {ia[1] + 4 * ia[2], ia[0] + 4 * ia[2], ia[0] + 4 * ia[1]};  // face point per dir
 
-    // ---- 1. state of this element
-    P uin[NV];
-    if (live) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            uin[v] = (P)A.u_in[v * m.npts + ec * NE + t];
-            sm.u[v][t] = uin[v];
-        }
-    }
-    long long nbr[3][2];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int s = 0; s < 2; ++s) nbr[d][s] = neighbour(m, ex, ey, ez, d, s);
-    __syncthreads();
-
-    // ---- 2. own and neighbour face values (3 dirs x 5 vars x 16 face pts)
-    if (live) {
-        for (int it = t; it < 240; it += 64) {
-            const int d = it / 80;
-            const int rem = it - d * 80;
-            const int v = rem >> 4, fp = rem & 15;
-            const P q0 = sm.u[v][line_pt(d, fp, 0)], q1 = sm.u[v][line_pt(d, fp, 1)];
-            const P q2 = sm.u[v][line_pt(d, fp, 2)], q3 = sm.u[v][line_pt(d, fp, 3)];
-            const P oL = trace4(q0, q1, q2, q3, A.tp.eL);
-            const P oR = trace4(q0, q1, q2, q3, A.tp.eR);
-            P nL, nR;
-            const P refl = (v > 0 && v < 4) ? (P)-1.0 : (P)1.0;
-            if (nbr[d][0] >= 0) {
-                P q[4];
-                load_line<S, P>(A.u_in + v * m.npts + nbr[d][0] * NE, d, fp, q);
-                nL = trace4(q[0], q[1], q[2], q[3], A.tp.eR);
-            } else {
-                nL = oL * refl;
-            }
-            if (nbr[d][1] >= 0) {
-                P q[4];
-                load_line<S, P>(A.u_in + v * m.npts + nbr[d][1] * NE, d, fp, q);
-                nR = trace4(q[0], q[1], q[2], q[3], A.tp.eL);
-            } else {
-                nR = oR * refl;
-            }
-            sm.tr[d][0][v][fp] = oL;
-            sm.tr[d][1][v][fp] = oR;
-            sm.nb[d][0][v][fp] = nL;
-            sm.nb[d][1][v][fp] = nR;
-        }
-    }
-    __syncthreads();
-
-    // ---- 3. corrected gradient at this point (BR1, rhs.cu:373-461)
-    C Dr[3][4];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int mm = 0; mm < 4; ++mm) Dr[d][mm] = A.tc.D[ia[d] * 4 + mm];
-    C gl[3], gr[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        gl[d] = A.tc.gL[ia[d]];
-        gr[d] = A.tc.gR[ia[d]];
-    }
-    C g[15];
+    // ---- P1: the element's x-lines (kept in registers for P2, P7, P10)
+    P ux[NV][4];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
+        if (live) {
+            ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, ux[v]);
+        } else {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const int fp = fpa[d];
-            C der = (C)0;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) der = fma(Dr[d][mm], (C)sm.u[v][line_pt(d, fp, mm)], der);
-            const P tl = sm.tr[d][0][v][fp], tr = sm.tr[d][1][v][fp];
-            const C jl = (C)((P)0.5 * (sm.nb[d][0][v][fp] + tl) - tl);
-            const C jr = (C)((P)0.5 * (sm.nb[d][1][v][fp] + tr) - tr);
-            C gv = der * A.jac[d];
-            gv += jl * gl[d] * A.jac[d];
-            gv += jr * gr[d] * A.jac[d];
-            if constexpr (sizeof(C) == 8) {
-                if (A.flags & kRoundQ) gv = (C)(float)gv;
-            }
-            g[3 * v + d] = gv;
-            sm.g[3 * v + d][t] = gv;
+            for (int a = 0; a < 4; ++a) ux[v][a] = (P)1.0;
         }
+        st4s(&sm.u[v][4 * l], ux[v]);
     }
+    const long long nxm = neighbour(m, ex, ey, ez, 0, 0), nxp = neighbour(m, ex, ey, ez, 0, 1);
+    const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
+    const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
     __syncthreads();
 
-    // ---- 4. face points: interface flux, own fluxes, corrections
-    if (live) {
-        for (int it = t; it < 96; it += 64) {
-            const int d = it >> 5, side = (it >> 4) & 1, fp = it & 15;
-            const bool wall = d == 1 && nbr[1][side] < 0;
-            if (d == 0)
-                face_point<FLUX, 0>(A, sm, ec, side, fp, wall);
-            else if (d == 1)
-                face_point<FLUX, 1>(A, sm, ec, side, fp, wall);
-            else
-                face_point<FLUX, 2>(A, sm, ec, side, fp, wall);
-        }
+    // ---- P2-P4: face values, gradient, interface fluxes per direction
+    line_pass<FLUX, 0>(A, sm, l, nxm, nxp, ux);
+    line_pass<FLUX, 1>(A, sm, l, nym, nyp, ux);
+    line_pass<FLUX, 2>(A, sm, l, nzm, nzp, ux);
+    __syncthreads();
+
+    // ---- P5-P6: viscous face fluxes of the y and z faces
+    face_grad_pass<1>(A, sm, ec, l, nym < 0, nyp < 0, live);
+    face_grad_pass<2>(A, sm, ec, l, false, false, live);
+    __syncthreads();
+
+    // ---- P7: pointwise fluxes of the x-line, x-divergence, x-face viscous flux
+    C divx[NV][4];
+    C gxL[15], gxR[15];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) divx[v][a] = (C)0;
+#pragma unroll
+    for (int c = 0; c < 15; ++c) {
+        gxL[c] = (C)0;
+        gxR[c] = (C)0;
     }
-    // ---- 5. volume fluxes at this point
-    C F[3][NV];
-    {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int p = 4 * l + i;
+        C g[15];
+#pragma unroll
+        for (int c = 0; c < 15; ++c) g[c] = sm.g[c][p];
+#pragma unroll
+        for (int c = 0; c < 15; ++c) {
+            if (!grad_used<0>(c)) continue;
+            gxL[c] = i == 0 ? g[c] * A.tc.eL[0] : fma(g[c], A.tc.eL[i], gxL[c]);
+            gxR[c] = i == 0 ? g[c] * A.tc.eR[0] : fma(g[c], A.tc.eR[i], gxR[c]);
+        }
         P qp[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) qp[v] = sm.u[v][t];
+        for (int v = 0; v < NV; ++v) qp[v] = ux[v][i];
         FaceState<C> s = make_face_state<C, P>(qp);
-        C praw = (C)raw_pressure<P>(qp[0], qp[1], qp[2], qp[3], qp[4]);
+        const C praw = (C)raw_pressure<P>(qp[0], qp[1], qp[2], qp[3], qp[4]);
+        C F[3][NV];
         volume_fluxes<C>(s, praw, g, A.mu, F);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) divx[v][a] = fma(A.tc.D[a * 4 + i], F[0][v], divx[v][a]);
+            sm.g[v][p] = F[1][v];
+            sm.g[5 + v][p] = F[2][v];
+        }
     }
-    __syncthreads();  // face points are done reading the gradient
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int v = 0; v < NV; ++v) sm.g[d * NV + v][t] = F[d][v];
+    viscous_face<0>(A, sm, ec, l, 0, gxL, live);
+    viscous_face<0>(A, sm, ec, l, 1, gxR, live);
     __syncthreads();
 
-    // ---- 6. divergence, lifting and the RK combination
+    // ---- P8-P9: y and z divergence along the lines
+    C* divz = reinterpret_cast<C*>(&sm.u[0][0]);
+    div_pass<1, C>(sm.g, &sm.g[10][0], l, A.tc.D, A.jac[1]);
+    div_pass<2, C>(&sm.g[5], divz, l, A.tc.D, A.jac[2]);
+    __syncthreads();
+
+    // ---- P10: RHS, lifting, RK combination
     if (!live) return;
-    P u0v[NV];
-    if (A.flags & kHasU0) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) u0v[v] = (P)A.u0[v * m.npts + ec * NE + t];
-    }
+    const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        C div = (C)0;
+        C dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
+        ld4s(&sm.g[10 + v][4 * l], dy);
+        ld4s(&divz[v * NE + 4 * l], dz);
+        ld4s(&sm.j[2][v][4 * lk], jy0);
+        ld4s(&sm.j[3][v][4 * lk], jy1);
+        ld4s(&sm.j[4][v][4 * lj], jz0);
+        ld4s(&sm.j[5][v][4 * lj], jz1);
+        const C jx0 = sm.j[0][v][l], jx1 = sm.j[1][v][l];
+        P u0v[4];
+        if (A.flags & kHasU0) ldg4<S, P>(A.u0 + v * m.npts + ec * NE + 4 * l, u0v);
+        P out[4];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const int fp = fpa[d];
-            const C* Fr = sm.g[d * NV + v];
-            C df = (C)0;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) df = fma(Dr[d][mm], Fr[line_pt(d, fp, mm)], df);
-            div += df * A.jac[d];
+        for (int i = 0; i < 4; ++i) {
+            C rvol = -((divx[v][i] * A.jac[0] + dy[i]) + dz[i]);
+            if (v == 1) rvol += A.forcing;
+            if constexpr (sizeof(C) == 8) {
+                if (A.flags & kRoundRhs) rvol = (C)(float)rvol;
+            }
+            const C cx = -(jx0 * A.tc.gL[i] * A.jac[0]) - (jx1 * A.tc.gR[i] * A.jac[0]);
+            const C cy = -(jy0[i] * A.tc.gL[lj] * A.jac[1]) - (jy1[i] * A.tc.gR[lj] * A.jac[1]);
+            const C cz = -(jz0[i] * A.tc.gL[lk] * A.jac[2]) - (jz1[i] * A.tc.gR[lk] * A.jac[2]);
+            const C rtot = rvol + (cx + cy + cz);
+            P o = A.rb * ux[v][i] + A.rc * (P)rtot;
+            if (A.flags & kHasU0) o = A.ra * u0v[i] + A.rb * ux[v][i] + A.rc * (P)rtot;
+            out[i] = o;
         }
-        C rvol = -div;
-        if (v == 1) rvol += A.forcing;
-        if constexpr (sizeof(C) == 8) {
-            if (A.flags & kRoundRhs) rvol = (C)(float)rvol;
-        }
-        C corr[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const int fp = fpa[d];
-            corr[d] = -(sm.j[d][0][v][fp] * gl[d] * A.jac[d]) - (sm.j[d][1][v][fp] * gr[d] * A.jac[d]);
-        }
-        const C rtot = rvol + (corr[0] + corr[1] + corr[2]);
-        P out = A.rb * uin[v] + A.rc * (P)rtot;
-        if (A.flags & kHasU0) out = A.ra * u0v[v] + A.rb * uin[v] + A.rc * (P)rtot;
-        A.u_out[v * m.npts + ec * NE + t] = (S)out;
+        stg4<S, P>(A.u_out + v * m.npts + ec * NE + 4 * l, out);
     }
 }
 
@@ -369,36 +498,60 @@ struct StageBParams {
     P rc;
 };
 
-// Phase B: u_out += rc * lift(-1/2 Fv_nbr) over the element's non-wall faces.
+// Phase B: u_out += rc * lift(-1/2 Fv_nbr) over the element's non-wall faces;
+// 16 threads per element, each the x-line l = j + 4k (128-bit accesses).
 template <class S, class P, class C, int EPB>
-__global__ void __launch_bounds__(64 * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
-    const int t = threadIdx.x & 63;
-    const long long e = (long long)blockIdx.x * EPB + (threadIdx.x >> 6);
+__global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
+    const int l = threadIdx.x & (LPE - 1);
+    const long long e = (long long)blockIdx.x * EPB + threadIdx.x / LPE;
     const Mesh& m = B.m;
     if (e >= m.nelem) return;
     const int ex = (int)(e % m.nx);
     const int ey = (int)((e / m.nx) % m.ny);
     const int ez = (int)(e / ((long long)m.nx * m.ny));
-    const int ia[3] = {t & 3, (t >> 2) & 3, t >> 4};
-    const int fpa[3] = {ia[1] + 4 * ia[2], ia[0] + 4 * ia[2], ia[0] + 4 * ia[1]};
-    C acc[4] = {(C)0, (C)0, (C)0, (C)0};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-            const long long nb = neighbour(m, ex, ey, ez, d, side);
-            if (nb < 0) continue;
-            const C w = (C)0.5 * B.jac[d] * (side ? B.tc.gR[ia[d]] : B.tc.gL[ia[d]]);
-            // the neighbour's record of the shared face is its opposite side
-            const C* src = B.fv + ((nb * 6 + 2 * d + (1 - side)) * 4) * NF + fpa[d];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) acc[v] = fma(w, __ldg(src + v * NF), acc[v]);
-        }
-    }
+    const int lj = l & 3, lk = l >> 2;
+    const long long nxm = neighbour(m, ex, ey, ez, 0, 0), nxp = neighbour(m, ex, ey, ez, 0, 1);
+    const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
+    const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
+    const C hx = (C)0.5 * B.jac[0], hy = (C)0.5 * B.jac[1], hz = (C)0.5 * B.jac[2];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        S* p = B.u_out + (v + 1) * m.npts + e * NE + t;
-        *p = (S)((P)*p + B.rc * (P)acc[v]);
+        C acc[4] = {(C)0, (C)0, (C)0, (C)0};
+        // the neighbour's record of the shared face is its opposite side
+        {
+            const C a0 = __ldg(B.fv + ((nxm * 6 + 1) * 4 + v) * NF + l);
+            const C a1 = __ldg(B.fv + ((nxp * 6 + 0) * 4 + v) * NF + l);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, fma(hx * B.tc.gR[i], a1, acc[i]));
+        }
+        if (nym >= 0) {
+            C w[4];
+            ld4s(B.fv + ((nym * 6 + 3) * 4 + v) * NF + 4 * lk, w);
+            const C c = hy * B.tc.gL[lj];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+        }
+        if (nyp >= 0) {
+            C w[4];
+            ld4s(B.fv + ((nyp * 6 + 2) * 4 + v) * NF + 4 * lk, w);
+            const C c = hy * B.tc.gR[lj];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+        }
+        {
+            C w0[4], w1[4];
+            ld4s(B.fv + ((nzm * 6 + 5) * 4 + v) * NF + 4 * lj, w0);
+            ld4s(B.fv + ((nzp * 6 + 4) * 4 + v) * NF + 4 * lj, w1);
+            const C c0 = hz * B.tc.gL[lk], c1 = hz * B.tc.gR[lk];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = fma(c0, w0[i], fma(c1, w1[i], acc[i]));
+        }
+        S* p = B.u_out + (v + 1) * m.npts + e * NE + 4 * l;
+        P cur[4];
+        ldc4<S, P>(p, cur);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) cur[i] = cur[i] + B.rc * (P)acc[i];
+        stg4<S, P>(p, cur);
     }
 }
 

@@ -164,9 +164,12 @@ def taylor_green_state(n, v0=0.1, gamma=1.4, length=2.0 * math.pi) -> list:
     return [rho, rho * u, rho * v, np.zeros_like(x), E]
 
 
-def tgv_dt(n, cfl=0.3, v0=0.1, length=2.0 * math.pi) -> float:
-    """Fixed dt at CFL 0.3 for the TGV case: cfl * (h/4) / (v0 + c0), c0 = 1."""
-    return cfl * (length / n / 4.0) / (v0 + 1.0)
+def tgv_dt(n, cfl=0.3, v0=0.1, length=2.0 * math.pi, order=3) -> float:
+    """Fixed dt of the TGV case at the given CFL number, with the usual FR/DG
+    definition dt = CFL * h / ((2P + 1) * lambda_max), h = element size,
+    lambda_max = v0 + c0 (c0 = 1). CFL 0.3 is stable with SSP-RK3 at P = 3
+    (0.4 is not)."""
+    return cfl * (length / n) / ((2 * order + 1) * (v0 + 1.0))
 
 
 def stack(planes, dtype) -> np.ndarray:

@@ -131,6 +131,9 @@ class Solver:
     def launches_per_step(self) -> int:
         return int(self._lib.od_launches_per_step(self._ctx))
 
+    def set_launch_shape(self, epb_a: int, epb_b: int) -> None:
+        self._chk(self._lib.od_set_launch_shape(self._ctx, int(epb_a), int(epb_b)), "od_set_launch_shape")
+
     def set_timing(self, enabled: bool) -> None:
         self._chk(self._lib.od_set_timing(self._ctx, int(enabled)), "od_set_timing")
 

@@ -1,0 +1,210 @@
+"""TEST INFRASTRUCTURE — Python side of the reference-kernel runner.
+
+``RefSolver`` runs the reference's own kernels (NVRTC-built from its sources
+by oracle/build_ref.py) with the reference host's launch shapes and step
+sequence (oracle/ref_harness.cpp). Used by the GPU parity tests, by the
+golden-fixture script and by ``bench.py --impl reference``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import time
+
+import numpy as np
+
+from .build_ref import HARNESS_SO, ptx_path
+
+
+class RefhParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("lx", ctypes.c_float), ("ly", ctypes.c_float), ("lz", ctypes.c_float),
+                ("y_wall", ctypes.c_int), ("u_f64", ctypes.c_int), ("rhs_f64", ctypes.c_int),
+                ("c_f64", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(HARNESS_SO):
+            raise FileNotFoundError(f"{HARNESS_SO} missing: run `python -m oracle.build`")
+        L = ctypes.CDLL(HARNESS_SO)
+        vp = ctypes.c_void_p
+        L.refh_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(RefhParams), ctypes.POINTER(vp)]
+        L.refh_destroy.argtypes = [vp]
+        L.refh_state_bytes.argtypes = [vp]
+        L.refh_state_bytes.restype = ctypes.c_size_t
+        L.refh_set_state.argtypes = [vp, vp, ctypes.c_size_t]
+        L.refh_get_state.argtypes = [vp, vp, ctypes.c_size_t]
+        L.refh_read.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t]
+        L.refh_rhs_stage.argtypes = [vp]
+        L.refh_rk.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.refh_swap.argtypes = [vp]
+        L.refh_step.argtypes = [vp, ctypes.c_int, ctypes.c_float]
+        L.refh_sync.argtypes = [vp]
+        L.refh_time_steps.argtypes = [vp, ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
+        L.refh_launches_per_step.argtypes = [vp]
+        L.refh_rk_block.argtypes = [vp]
+        L.refh_last_error.argtypes = [vp]
+        L.refh_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+class RefSolver:
+    """The reference's kernels on one GPU, driven like src/solver.rs."""
+
+    def __init__(self, nx, ny, nz, lx, ly, lz, flux="slau2", y_wall=True, u="f32", q=None, rhs=None,
+                 compute=None, fast_math=True, device=0):
+        q = q or u
+        rhs = rhs or u
+        compute = compute or u
+        path = ptx_path(u, q, rhs, compute, flux, y_wall, fast_math)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `python -m oracle.build_ref` where the reference tree exists")
+        self.L = lib()
+        self.p = RefhParams(nx, ny, nz, np.float32(lx), np.float32(ly), np.float32(lz), int(y_wall),
+                            int(u == "f64"), int(rhs == "f64"), int(compute == "f64"), device)
+        self.h = ctypes.c_void_p()
+        rc = self.L.refh_create(path.encode(), ctypes.byref(self.p), ctypes.byref(self.h))
+        if rc != 0:
+            msg = self.L.refh_last_error(self.h).decode() if self.h.value else "driver unavailable"
+            self.close()
+            raise RuntimeError(f"refh_create failed: {msg}")
+        self.udt = np.float64 if u == "f64" else np.float32
+        self.rdt = np.float64 if rhs == "f64" else np.float32
+        self.cdt = np.float64 if compute == "f64" else np.float32
+        self.nelem = nx * ny * nz
+        self.npts = self.nelem * 64
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.refh_destroy(self.h)
+        self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc}): {self.L.refh_last_error(self.h).decode()}")
+
+    def set_state(self, u):
+        u = np.ascontiguousarray(u, dtype=self.udt)
+        self._ck(self.L.refh_set_state(self.h, u.ctypes.data_as(ctypes.c_void_p), u.nbytes), "refh_set_state")
+
+    def get_state(self):
+        out = np.empty(5 * self.npts, dtype=self.udt)
+        self._ck(self.L.refh_get_state(self.h, out.ctypes.data_as(ctypes.c_void_p), out.nbytes), "refh_get_state")
+        return out
+
+    def read(self, which):
+        if which <= 1:
+            out = np.empty(5 * self.npts, dtype=self.udt)
+        elif which == 2:
+            out = np.empty(5 * self.npts, dtype=self.rdt)
+        elif which < 9:
+            out = np.empty(self.nelem * 16 * 12, dtype=self.cdt)
+        else:
+            out = np.empty(self.nelem * 16 * 5, dtype=self.cdt)
+        self._ck(self.L.refh_read(self.h, which, out.ctypes.data_as(ctypes.c_void_p), out.nbytes), "refh_read")
+        return out
+
+    def rhs_stage(self):
+        self._ck(self.L.refh_rhs_stage(self.h), "refh_rhs_stage")
+
+    def rk(self, stage1, a, b, c):
+        self._ck(self.L.refh_rk(self.h, int(stage1), a, b, c), "refh_rk")
+
+    def swap(self):
+        self.L.refh_swap(self.h)
+
+    def step(self, n, dt):
+        self._ck(self.L.refh_step(self.h, int(n), float(np.float32(dt))), "refh_step")
+
+    def sync(self):
+        self._ck(self.L.refh_sync(self.h), "refh_sync")
+
+    def time_steps(self, n, dt) -> float:
+        ms = ctypes.c_float()
+        self._ck(self.L.refh_time_steps(self.h, int(n), float(np.float32(dt)), ctypes.byref(ms)), "refh_time_steps")
+        return float(ms.value)
+
+    @property
+    def launches_per_step(self):
+        return int(self.L.refh_launches_per_step(self.h))
+
+    @property
+    def rk_block(self):
+        """Threads per block of the RK launches (1024 as cudarc, unless the
+        kernel cannot launch that many on this GPU)."""
+        return int(self.L.refh_rk_block(self.h))
+
+    @property
+    def state_bytes(self):
+        return int(self.L.refh_state_bytes(self.h))
+
+
+def bench_line(args, w, rk_per_step, metric, bytes_per_dof_stage) -> dict:
+    """``bench.py --impl reference``: the reference's own kernels on this GPU,
+    same workload, metric and step definition as the project's arm."""
+    import math
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench  # noqa: WPS433
+    try:
+        import torch
+        torch.cuda.init()
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        u = bench.build_state(np.float32)
+        npts = w["nx"] * w["ny"] * w["nz"] * 64
+        with RefSolver(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"], w["lz"], w["flux"], w["y_wall"], "f32",
+                       device=local) as r:
+            r.set_state(u)
+            r.time_steps(rk_per_step * args.warmup, w["dt"])
+            clocks = bench.ClockSampler(local)
+            clocks.start()
+            ms = r.time_steps(rk_per_step * args.steps, w["dt"])
+            clk = clocks.stop()
+            # e2e: state upload + 50 steps + download per bench step
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                r.set_state(u)
+                r.step(rk_per_step, w["dt"])
+                out = r.get_state()
+            e2e_s = time.perf_counter() - t0
+            launches = r.launches_per_step * rk_per_step * args.steps
+            finite = bool(np.isfinite(out).all())
+        stages = args.steps * rk_per_step * 3
+        value = npts * stages / (ms / 1e3) / 1e9
+        e2e = npts * stages / e2e_s / 1e9
+        return {
+            "impl": "reference", "metric": metric, "value": round(value, 3), "unit": "Gdof*stage/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (channel IC generator: laminar profile + Fourier trip, seed 42)",
+            "config": {"workload": "channel 48^3 elements, FR P=3 (7,077,888 dofs), SLAU2, y slip walls, f32",
+                       "rk3_steps_per_step": rk_per_step, "dt": float(np.float32(w["dt"])),
+                       "implementation": "reference CUDA sources, NVRTC compute_100 --use_fast_math, "
+                                         "driver JIT, solver.rs launch shapes and sequence",
+                       "l2": "inputs larger than L2"},
+            "e2e": {"value": round(e2e, 3), "unit": "Gdof*stage/s", "h2d_bytes_per_step": int(u.nbytes),
+                    "d2h_bytes_per_step": int(u.nbytes)},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Gdof*stage/s", "cores": 0, "kind": "reference",
+                             "sample": "the reference has no CPU path: its own CUDA kernels on this GPU, "
+                                       f"{args.steps} x {rk_per_step} RK3 steps"},
+            "gpu_launches": launches, "clocks": clk, "state_finite": finite,
+        }
+    except Exception as exc:
+        return {"impl": "reference", "unavailable": f"reference kernels could not run: {exc}"}

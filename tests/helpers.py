@@ -44,3 +44,20 @@ def random_smooth(nx, ny, nz, seed=0, dtype=np.float64, amp=0.05) -> np.ndarray:
 
 def tgv(n, dtype=np.float64) -> np.ndarray:
     return ic.stack(ic.taylor_green_state(n), dtype)
+
+
+def assert_f32_parity(got, ref, truth, bar=1e-5, slack=2.0, floor=1e-6):
+    """f32 parity between two f32 implementations (got, ref) of the same run.
+
+    rho, rho*u and E (O(1) planes) must agree within ``bar`` relative L2.
+    rho*v and rho*w are O(1e-2) planes whose f32 round-off (absolute ~1e-7
+    from the pressure gradient) is already ~1e-5..1e-4 *relative*; for every
+    plane ``got`` must be no further from the f64 solution ``truth`` than
+    ``slack`` times the reference's own distance (or ``floor``)."""
+    e_pair = rel_l2(got, ref)
+    e_got = rel_l2(got, truth)
+    e_ref = rel_l2(ref, truth)
+    big = [0, 1, 4]
+    assert np.all(e_pair[big] < bar), ("O(1) planes differ", e_pair)
+    assert np.all(e_got <= np.maximum(slack * e_ref, floor)), ("less accurate than the reference in f32", e_got, e_ref)
+    return e_pair, e_got, e_ref

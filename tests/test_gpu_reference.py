@@ -1,0 +1,147 @@
+"""Parity against the reference's own kernels (NVRTC-built from its CUDA
+sources, launched like src/solver.rs) on identical initial states.
+
+Bars (relative L2 per variable after 100 steps): f64 pipeline 1e-10,
+f32 pipeline 1e-5. Also pins the CPU oracle kernel by kernel.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import assert_f32_parity, channel_trip, random_smooth, rel_l2, tgv
+from opendynamo_b200.initial_state import tgv_dt
+from opendynamo_b200.solver import Solver, make_params
+
+BOX = (2 * math.pi, 2.0, math.pi)
+
+
+def _ref():
+    from oracle.ref_harness import RefSolver
+    return RefSolver
+
+
+@pytest.mark.gpu
+def test_tgv_f64_100_steps_vs_reference():
+    """Config 1: TGV 8^3, Rusanov, periodic, f64 pipeline, CFL 0.3, 100 steps."""
+    n = 8
+    L = 2 * math.pi
+    u = tgv(n)
+    dt = float(np.float32(tgv_dt(n)))
+    with _ref()(n, n, n, L, L, L, "rusanov", False, "f64") as r:
+        r.set_state(u)
+        r.step(100, dt)
+        ref = r.get_state()
+    with Solver(make_params(n, n, n, L, L, L, "rusanov", False, "f64")) as s:
+        s.set_state(u)
+        s.step(100, dt)
+        got = s.get_state()
+    err = rel_l2(got, ref)
+    assert np.all(err < 1e-10), err
+    assert np.all(rel_l2(got - u, ref - u) < 1e-8)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mesh", [(12, 8, 6), (48, 48, 48)])
+def test_channel_f32_100_steps_vs_reference(mesh):
+    """Config 2 physics (channel, SLAU2, y walls, f32, the reference's
+    fast-math build): 100 steps from the same IC. The f64 truth is this
+    project's f64 pipeline (itself held to 1e-10 of the reference's f64)."""
+    u = channel_trip(*mesh, amp=0.01, dtype=np.float32)
+    dt = 2e-4
+    with _ref()(*mesh, *BOX, "slau2", True, "f32") as r:
+        r.set_state(u)
+        r.step(100, dt)
+        ref = r.get_state()
+    with Solver(make_params(*mesh, *BOX, "slau2", True, "f32")) as s:
+        s.set_state(u)
+        s.step(100, float(np.float32(dt)))
+        got = s.get_state()
+    with Solver(make_params(*mesh, *BOX, "slau2", True, "f64")) as s:
+        s.set_state(u.astype(np.float64))
+        s.step(100, float(np.float32(dt)))
+        truth = s.get_state()
+    e_pair, e_got, e_ref = assert_f32_parity(got, ref, truth)
+    print("f32 vs reference", e_pair, "ours vs f64", e_got, "reference vs f64", e_ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flux", ["slau2", "ausm+", "rusanov"])
+@pytest.mark.parametrize("wall", [True, False])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_steps_vs_reference(prec, wall, flux):
+    mesh = (4, 3, 5)
+    dtype = np.float64 if prec == "f64" else np.float32
+    u = channel_trip(*mesh, amp=0.02, dtype=dtype)
+    dt = 1e-3
+    with _ref()(*mesh, *BOX, flux, wall, prec) as r:
+        r.set_state(u)
+        r.step(20, dt)
+        ref = r.get_state()
+    with Solver(make_params(*mesh, *BOX, flux, wall, prec)) as s:
+        s.set_state(u)
+        s.step(20, float(np.float32(dt)))
+        got = s.get_state()
+    if prec == "f64":
+        assert np.all(rel_l2(got, ref) < 1e-12), rel_l2(got, ref)
+        assert np.all(rel_l2(got - u, ref - u) < 1e-9)
+    else:
+        with Solver(make_params(*mesh, *BOX, flux, wall, "f64")) as s:
+            s.set_state(u.astype(np.float64))
+            s.step(20, float(np.float32(dt)))
+            truth = s.get_state()
+        assert_f32_parity(got, ref, truth)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flux", ["slau2", "ausm+", "rusanov"])
+@pytest.mark.parametrize("wall", [True, False])
+def test_oracle_kernels_vs_reference_f64(flux, wall):
+    """Kernel by kernel: volume RHS + slices, face corrections, RK stage."""
+    mesh = (3, 4, 2)
+    u = random_smooth(*mesh, seed=7)
+    op = oracle.make_params(*mesh, *BOX, flux=flux, y_wall=wall, u="f64")
+    with _ref()(*mesh, *BOX, flux, wall, "f64") as r:
+        r.set_state(u)
+        r.rhs_stage()
+        rhs_ref = r.read(2)
+        sl_ref = [r.read(3 + q) for q in range(6)]
+        j_ref = [r.read(9 + q) for q in range(6)]
+        r.rk(True, 1.0, 0.0, 1e-3)
+        r.sync()
+        up_ref = r.read(1)
+    rhs, sl = oracle.volume(op, u)
+    assert rel_l2(rhs, rhs_ref).max() < 1e-12
+    for a, b in zip(sl, sl_ref):
+        assert np.abs(a - b).max() <= 1e-12 * max(1.0, np.abs(b).max())
+    j = oracle.faces(op, u, sl_ref)
+    for a, b in zip(j, j_ref):
+        assert np.abs(a - b).max() <= 1e-11 * max(1.0, np.abs(b).max())
+    dst = np.zeros_like(u)
+    oracle.rk(op, dst, u, rhs_ref, j_ref, 1.0, 0.0, 1e-3, True)
+    assert rel_l2(dst - u, up_ref - u).max() < 1e-12
+
+
+@pytest.mark.gpu
+def test_reference_default_precision_vs_reference():
+    """u_real = f64 with q/rhs/compute = f32 (constants.cuh defaults)."""
+    mesh = (4, 3, 5)
+    u = channel_trip(*mesh, amp=0.02)
+    with _ref()(*mesh, *BOX, "slau2", True, "f64", q="f32", rhs="f32", compute="f32") as r:
+        r.set_state(u)
+        r.step(20, 1e-3)
+        ref = r.get_state()
+    with Solver(make_params(*mesh, *BOX, "slau2", True, "f64", q_real="f32", rhs_real="f32",
+                            compute_real="f32")) as s:
+        s.set_state(u)
+        s.step(20, float(np.float32(1e-3)))
+        got = s.get_state()
+    with Solver(make_params(*mesh, *BOX, "slau2", True, "f64")) as s:
+        s.set_state(u)
+        s.step(20, float(np.float32(1e-3)))
+        truth = s.get_state()
+    assert_f32_parity(got, ref, truth)
