@@ -53,7 +53,8 @@ typedef struct od_params {
     int u_real, q_real, rhs_real, compute_real; /* OD_F32 / OD_F64 ([precision] table) */
     int mixed;                     /* 1 = precision form: f64 state, RK and pressure recovery with
                                       f32 fluxes; requires u_real = f64, compute_real = f32 */
-    int fast_math;                 /* accepted for config parity ([solver] fast_math) */
+    int fast_math;                 /* 1 = approximate f32 division / square root, as the reference's
+                                      default --use_fast_math build ([solver] fast_math); f64 unaffected */
     double mu;                     /* dynamic viscosity; reference constant 1.6e-4 (constants.cuh:42) */
     double forcing;                /* source added to the rho*u RHS; reference 1e-3 (rhs.cu:508) */
     int device;                    /* CUDA device ordinal */
@@ -106,7 +107,7 @@ void* od_stream(od_ctx* ctx);
 /* Kernel launches od_step enqueues per step (for launch accounting). */
 int od_launches_per_step(const od_ctx* ctx);
 
-/* Launch shape: elements per thread block of the phase-A kernel (2, 4 or 8;
+/* Launch shape: elements per thread block of the phase-A kernel (2 or 4;
  * 16 threads per element) and of the phase-B kernel (8 or 16). Results do
  * not depend on it; the autotuner picks it per mesh and precision. */
 int od_set_launch_shape(od_ctx* ctx, int elems_per_block_a, int elems_per_block_b);

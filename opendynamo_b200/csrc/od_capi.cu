@@ -115,6 +115,7 @@ struct od_ctx {
     cudaStream_t stream = nullptr;
     void* U[3] = {nullptr, nullptr, nullptr};
     void* fv = nullptr;
+    void* rhs = nullptr;      // deferred RK combination: RHS between phase A and phase B
     size_t state_bytes = 0;
     size_t elem_size = 4;
     long long nelem = 0;
@@ -154,6 +155,8 @@ int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, doub
     L.u0 = u0;
     L.u_out = u_out;
     L.fv = c->fv;
+    L.rhs = c->rhs;
+    L.fast_math = c->p.fast_math != 0;
     L.nx = c->p.nx;
     L.ny = c->p.ny;
     L.nz = c->p.nz;
@@ -280,6 +283,15 @@ int od_create(const od_params* p, od_ctx** out) {
             return cuda_fail(c, e, "cudaMalloc state");
         }
     }
+    // An f32 state is rounded once per stage: with the viscous phase B the RK
+    // combination moves there and phase A hands over the RHS.
+    if (!c->fns.s_double && p->mu != 0.0) {
+        e = cudaMalloc(&c->rhs, c->state_bytes);
+        if (e != cudaSuccess) {
+            *out = c;
+            return cuda_fail(c, e, "cudaMalloc RHS buffer");
+        }
+    }
     const size_t fv_bytes = (size_t)nelem * 6 * 4 * 16 * (c->fns.c_double ? 8 : 4);
     e = cudaMalloc(&c->fv, fv_bytes);
     if (e != cudaSuccess) {
@@ -303,6 +315,7 @@ void od_destroy(od_ctx* c) {
     for (int b = 0; b < 3; ++b)
         if (c->U[b]) cudaFree(c->U[b]);
     if (c->fv) cudaFree(c->fv);
+    if (c->rhs) cudaFree(c->rhs);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -375,7 +388,8 @@ int od_rhs(od_ctx* c, void* d_out, size_t bytes) {
     if (!c || !d_out) return OD_ERR_ARG;
     if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "RHS size does not match the mesh");
     if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
-    if (d_out == c->U[0]) return fail(c, OD_ERR_ARG, "RHS output must not alias the state");
+    if (d_out == c->U[0] || (c->rhs && d_out == c->rhs))
+        return fail(c, OD_ERR_ARG, "RHS output must not alias the state");
     if (int rc = set_device(c)) return rc;
     return enqueue_stage(c, c->U[0], nullptr, d_out, 0.0, 0.0, 1.0);
 }
@@ -397,8 +411,8 @@ int od_launches_per_step(const od_ctx* c) {
 
 int od_set_launch_shape(od_ctx* c, int elems_per_block_a, int elems_per_block_b) {
     if (!c) return OD_ERR_ARG;
-    if (elems_per_block_a != 2 && elems_per_block_a != 4 && elems_per_block_a != 8)
-        return fail(c, OD_ERR_ARG, "phase-A elements per block must be 2, 4 or 8");
+    if (elems_per_block_a != 2 && elems_per_block_a != 4)
+        return fail(c, OD_ERR_ARG, "phase-A elements per block must be 2 or 4");
     if (elems_per_block_b != 8 && elems_per_block_b != 16)
         return fail(c, OD_ERR_ARG, "phase-B elements per block must be 8 or 16");
     c->epb_a = elems_per_block_a;

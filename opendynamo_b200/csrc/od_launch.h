@@ -11,6 +11,7 @@ enum StageFlags : int {
     kHasU0 = 1,      // out = ra*u0 + rb*u_in + rc*R (else rb*u_in + rc*R)
     kRoundQ = 2,     // round the gradient through f32 (q_real = f32 with f64 compute)
     kRoundRhs = 4,   // round the volume RHS through f32 (rhs_real = f32 with f64 compute)
+    kDeferRK = 8,    // phase A stores the RHS, phase B performs the RK combination
 };
 
 // FR operator tables in double (the host computes them once, as
@@ -24,6 +25,7 @@ struct StageLaunch {
     const void* u0;      // null on stage 1 / single RHS evaluations
     void* u_out;
     void* fv;            // viscous face buffer
+    void* rhs;           // RHS buffer of the deferred RK combination (null otherwise)
     int nx, ny, nz, y_wall;
     long long nelem;
     TablesD tab;
@@ -33,6 +35,7 @@ struct StageLaunch {
     int flags;           // kHasU0 | kRoundQ | kRoundRhs
     int flux;            // 0 slau2, 1 ausm+, 2 rusanov
     int epb_a, epb_b;    // elements per block of phase A / phase B
+    bool fast_math;      // approximate f32 division / square root (the reference's default build)
     bool phase_b;        // launch phase B (viscous neighbour term)
     cudaEvent_t ev[3];   // optional timing events: before A, between A and B, after B
 };

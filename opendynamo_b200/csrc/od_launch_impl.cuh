@@ -20,20 +20,26 @@ Tab<T> cast_tab(const TablesD& t) {
     return r;
 }
 
-template <class S, class P, class C, int FLUX, int EPB>
+template <class S, class P, class C, class M, int FLUX, int EPB>
 cudaError_t launch_a(const StageAParams<S, P, C>& A, long long nelem, cudaStream_t s) {
     const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
     const size_t smem = sizeof(SlotA<P, C>) * EPB;
-    stage_a_kernel<S, P, C, FLUX, EPB><<<grid, LPE * EPB, smem, s>>>(A);
+    stage_a_kernel<S, P, C, M, FLUX, EPB><<<grid, LPE * EPB, smem, s>>>(A);
     return cudaGetLastError();
 }
 
-template <class S, class P, class C, int FLUX>
+template <class S, class P, class C, class M, int FLUX>
 cudaError_t launch_a_epb(const StageAParams<S, P, C>& A, long long nelem, int epb, cudaStream_t s) {
-    switch (epb) {
-        case 2: return launch_a<S, P, C, FLUX, 2>(A, nelem, s);
-        case 8: return launch_a<S, P, C, FLUX, 8>(A, nelem, s);
-        default: return launch_a<S, P, C, FLUX, 4>(A, nelem, s);
+    if (epb == 2) return launch_a<S, P, C, M, FLUX, 2>(A, nelem, s);
+    return launch_a<S, P, C, M, FLUX, 4>(A, nelem, s);
+}
+
+template <class S, class P, class C, class M>
+cudaError_t launch_a_flux(const StageAParams<S, P, C>& A, int flux, long long nelem, int epb, cudaStream_t s) {
+    switch (flux) {
+        case kSlau2: return launch_a_epb<S, P, C, M, kSlau2>(A, nelem, epb, s);
+        case kAusmPlus: return launch_a_epb<S, P, C, M, kAusmPlus>(A, nelem, epb, s);
+        default: return launch_a_epb<S, P, C, M, kRusanov>(A, nelem, epb, s);
     }
 }
 
@@ -44,12 +50,16 @@ cudaError_t launch_b(const StageBParams<S, P, C>& B, long long nelem, cudaStream
     return cudaGetLastError();
 }
 
+// fast math changes only f32 arithmetic: f64-compute combinations use one variant
+template <class C>
+constexpr bool has_fast_variant() { return sizeof(C) == 4; }
+
 template <class S, class P, class C>
 cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     StageAParams<S, P, C> A;
     A.u_in = (const S*)L.u_in;
     A.u0 = (const S*)L.u0;
-    A.u_out = (S*)L.u_out;
+    A.u_out = (S*)(L.rhs ? L.rhs : L.u_out);
     A.fv = (C*)L.fv;
     A.m.nx = L.nx;
     A.m.ny = L.ny;
@@ -65,54 +75,69 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.rc = (P)L.rc;
     A.mu = (C)L.mu;
     A.forcing = (C)L.forcing;
-    A.flags = L.flags;
+    A.flags = L.flags | (L.rhs ? kDeferRK : 0);
     if (L.ev[0]) cudaEventRecord(L.ev[0], s);
     cudaError_t err;
-    switch (L.flux) {
-        case kSlau2: err = launch_a_epb<S, P, C, kSlau2>(A, L.nelem, L.epb_a, s); break;
-        case kAusmPlus: err = launch_a_epb<S, P, C, kAusmPlus>(A, L.nelem, L.epb_a, s); break;
-        default: err = launch_a_epb<S, P, C, kRusanov>(A, L.nelem, L.epb_a, s); break;
+    if constexpr (has_fast_variant<C>()) {
+        if (L.fast_math)
+            err = launch_a_flux<S, P, C, MathFast>(A, L.flux, L.nelem, L.epb_a, s);
+        else
+            err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, L.nelem, L.epb_a, s);
+    } else {
+        err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, L.nelem, L.epb_a, s);
     }
     if (err != cudaSuccess) return err;
     if (L.ev[1]) cudaEventRecord(L.ev[1], s);
     if (L.phase_b) {
         StageBParams<S, P, C> B;
         B.u_out = (S*)L.u_out;
+        B.rhs = (const S*)L.rhs;
+        B.u_in = (const S*)L.u_in;
+        B.u0 = (const S*)L.u0;
         B.fv = (const C*)L.fv;
         B.m = A.m;
         B.tc = A.tc;
         for (int d = 0; d < 3; ++d) B.jac[d] = A.jac[d];
+        B.ra = A.ra;
+        B.rb = A.rb;
         B.rc = A.rc;
-        switch (L.epb_b) {
-            case 8: err = launch_b<S, P, C, 8>(B, L.nelem, s); break;
-            default: err = launch_b<S, P, C, 16>(B, L.nelem, s); break;
-        }
+        B.flags = A.flags;
+        if (L.epb_b == 8)
+            err = launch_b<S, P, C, 8>(B, L.nelem, s);
+        else
+            err = launch_b<S, P, C, 16>(B, L.nelem, s);
         if (err != cudaSuccess) return err;
     }
     if (L.ev[2]) cudaEventRecord(L.ev[2], s);
     return cudaSuccess;
 }
 
-template <class S, class P, class C, int FLUX>
+template <class S, class P, class C, class M, int FLUX>
 cudaError_t prepare_flux() {
-    cudaError_t e;
-    e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(SlotA<P, C>) * 2));
+    cudaError_t e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, M, FLUX, 2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(SlotA<P, C>) * 2));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(SlotA<P, C>) * 4));
+    return cudaFuncSetAttribute(stage_a_kernel<S, P, C, M, FLUX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(SlotA<P, C>) * 4));
+}
+
+template <class S, class P, class C, class M>
+cudaError_t prepare_m() {
+    cudaError_t e = prepare_flux<S, P, C, M, kSlau2>();
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(stage_a_kernel<S, P, C, FLUX, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(SlotA<P, C>) * 8));
+    e = prepare_flux<S, P, C, M, kAusmPlus>();
+    if (e != cudaSuccess) return e;
+    return prepare_flux<S, P, C, M, kRusanov>();
 }
 
 template <class S, class P, class C>
 cudaError_t prepare_t() {
-    cudaError_t e = prepare_flux<S, P, C, kSlau2>();
-    if (e != cudaSuccess) return e;
-    e = prepare_flux<S, P, C, kAusmPlus>();
-    if (e != cudaSuccess) return e;
-    return prepare_flux<S, P, C, kRusanov>();
+    cudaError_t e = prepare_m<S, P, C, MathIeee>();
+    if constexpr (has_fast_variant<C>()) {
+        if (e == cudaSuccess) e = prepare_m<S, P, C, MathFast>();
+    }
+    return e;
 }
 
 }  // namespace od

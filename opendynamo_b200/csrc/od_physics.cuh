@@ -20,6 +20,48 @@ namespace od {
 
 enum Flux : int { kSlau2 = 0, kAusmPlus = 1, kRusanov = 2 };
 
+// Division / reciprocal / square root policy. MathIeee: correctly rounded
+// (the reference with fast_math = false, and every f64 operation).
+// MathFast: for f32 operands the approximate PTX forms (rcp.approx,
+// sqrt.approx, ~1-2 ulp), the arithmetic of the reference's default
+// --use_fast_math build; f64 operands stay IEEE (fast math does not touch them).
+struct MathIeee {
+    template <class T>
+    static __device__ __forceinline__ T rcp(T x) { return (T)1.0 / x; }
+    template <class T>
+    static __device__ __forceinline__ T div(T a, T b) { return a / b; }
+    template <class T>
+    static __device__ __forceinline__ T sqrt(T x) { return ::sqrt(x); }
+};
+
+struct MathFast {
+    template <class T>
+    static __device__ __forceinline__ T rcp(T x) {
+        if constexpr (sizeof(T) == 4) {
+            float r;
+            asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+            return r;
+        } else {
+            return (T)1.0 / x;
+        }
+    }
+    template <class T>
+    static __device__ __forceinline__ T div(T a, T b) {
+        if constexpr (sizeof(T) == 4) return a * rcp(b);
+        else return a / b;
+    }
+    template <class T>
+    static __device__ __forceinline__ T sqrt(T x) {
+        if constexpr (sizeof(T) == 4) {
+            float r;
+            asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+            return r;
+        } else {
+            return ::sqrt(x);
+        }
+    }
+};
+
 template <class C>
 struct Gas {
     static __device__ __forceinline__ C gamma() { return (C)1.4; }
@@ -33,9 +75,9 @@ template <class C>
 __device__ __forceinline__ C cmin(C a, C b) { return a < b ? a : b; }
 
 // Raw pressure (gamma-1)(E - |m|^2 / (2 rho)); the viscous flux uses it unclamped.
-template <class P>
+template <class M, class P>
 __device__ __forceinline__ P raw_pressure(P r, P m0, P m1, P m2, P E) {
-    P ke = (P)0.5 * (m0 * m0 + m1 * m1 + m2 * m2) / r;
+    P ke = M::div((P)0.5 * (m0 * m0 + m1 * m1 + m2 * m2), r);
     return Gas<P>::gm1() * (E - ke);
 }
 
@@ -52,14 +94,15 @@ struct FaceState {
     C p;   // clamped
 };
 
-template <class C, class P>
-__device__ __forceinline__ FaceState<C> make_face_state(const P* qp) {
+template <class M, class C, class P>
+__device__ __forceinline__ FaceState<C> make_face_state(const P* qp, C& praw_out) {
     FaceState<C> s;
 #pragma unroll
     for (int v = 0; v < 5; ++v) s.q[v] = (C)qp[v];
-    P praw = raw_pressure<P>(qp[0], qp[1], qp[2], qp[3], qp[4]);
+    P praw = raw_pressure<M, P>(qp[0], qp[1], qp[2], qp[3], qp[4]);
+    praw_out = (C)praw;
     s.p = clamp_p<C>((C)praw);
-    s.ir = (C)1.0 / s.q[0];
+    s.ir = M::rcp(s.q[0]);
     s.vel[0] = s.q[1] * s.ir;
     s.vel[1] = s.q[2] * s.ir;
     s.vel[2] = s.q[3] * s.ir;
@@ -78,9 +121,21 @@ __device__ __forceinline__ void euler_flux(const FaceState<C>& s, C* f) {
     f[4] = vn * (s.q[4] + s.p);
 }
 
+// Inviscid flux along axis d (d known after unrolling).
 template <class C>
+__device__ __forceinline__ void euler_flux_dyn(const FaceState<C>& s, int d, C* f) {
+    C vn = s.vel[d];
+    f[0] = s.q[1 + d];
+    f[1] = s.q[1] * vn;
+    f[2] = s.q[2] * vn;
+    f[3] = s.q[3] * vn;
+    f[1 + d] += s.p;
+    f[4] = vn * (s.q[4] + s.p);
+}
+
+template <class M, class C>
 __device__ __forceinline__ C sound_speed(C p, C r) {
-    return sqrt(cmax((C)0.0, Gas<C>::gamma() * p / cmax((C)1e-7, r)));
+    return M::sqrt(cmax((C)0.0, M::div(Gas<C>::gamma() * p, cmax((C)1e-7, r))));
 }
 
 // Viscous flux along axis D at a face point from the state and the
@@ -143,21 +198,23 @@ __device__ __forceinline__ void volume_fluxes(const FaceState<C>& s, C praw, con
         C dke = (s.q[1] * g[3 + d] + s.q[2] * g[6 + d] + s.q[3] * g[9 + d]) * ir - ke * g[d] * ir;
         C dp = Gas<C>::gm1() * (g[12 + d] - dke);
         C heat = -kappa * (dp * ir - praw * g[d] * ir * ir);
-        out[d][0] = s.q[1 + d];
-        out[d][1] = s.q[1] * vn - tau[0][d];
-        out[d][2] = s.q[2] * vn - tau[1][d];
-        out[d][3] = s.q[3] * vn - tau[2][d];
-        out[d][1 + d] += s.p;
-        out[d][4] = vn * (s.q[4] + s.p) - (s.vel[0] * tau[0][d] + s.vel[1] * tau[1][d] + s.vel[2] * tau[2][d] - heat);
+        // (F_euler) - (F_viscous), each formed first as the reference does
+        C fe[5];
+        euler_flux_dyn(s, d, fe);
+        out[d][0] = fe[0];
+        out[d][1] = fe[1] - tau[0][d];
+        out[d][2] = fe[2] - tau[1][d];
+        out[d][3] = fe[3] - tau[2][d];
+        out[d][4] = fe[4] - (s.vel[0] * tau[0][d] + s.vel[1] * tau[1][d] + s.vel[2] * tau[2][d] - heat);
     }
 }
 
 // ---- interface fluxes (axis-aligned normal D, left state L, right state R) ----
 
-template <int D, class C>
+template <class M, int D, class C>
 __device__ __forceinline__ void rusanov(const FaceState<C>& L, const FaceState<C>& R, C* f) {
     C vnL = L.vel[D], vnR = R.vel[D];
-    C smax = cmax(fabs(vnL) + sound_speed(L.p, L.q[0]), fabs(vnR) + sound_speed(R.p, R.q[0]));
+    C smax = cmax(fabs(vnL) + sound_speed<M>(L.p, L.q[0]), fabs(vnR) + sound_speed<M>(R.p, R.q[0]));
     C fL[5], fR[5];
     euler_flux<D>(L, fL);
     euler_flux<D>(R, fR);
@@ -165,11 +222,11 @@ __device__ __forceinline__ void rusanov(const FaceState<C>& L, const FaceState<C
     for (int v = 0; v < 5; ++v) f[v] = (C)0.5 * (fL[v] + fR[v] - smax * (R.q[v] - L.q[v]));
 }
 
-template <int D, class C>
+template <class M, int D, class C>
 __device__ __forceinline__ void ausm_plus(const FaceState<C>& L, const FaceState<C>& R, C* f) {
     const C alpha = (C)0.1875, beta = (C)0.125;
-    C cm = cmax(sound_speed(L.p, L.q[0]), sound_speed(R.p, R.q[0]));
-    C icm = (C)1.0 / cm;
+    C cm = cmax(sound_speed<M>(L.p, L.q[0]), sound_speed<M>(R.p, R.q[0]));
+    C icm = M::rcp(cm);
     C mL = L.vel[D] * icm, mR = R.vel[D] * icm;
     C mp, pp, mm, pm;
     if (fabs(mL) >= (C)1.0) {
@@ -201,20 +258,20 @@ __device__ __forceinline__ void ausm_plus(const FaceState<C>& L, const FaceState
     f[4] = mdot * ((W.q[4] + W.p) * W.ir);
 }
 
-template <int D, class C>
+template <class M, int D, class C>
 __device__ __forceinline__ void slau2(const FaceState<C>& L, const FaceState<C>& R, C* f) {
     C rL = L.q[0], rR = R.q[0];
     C vnL = L.vel[D], vnR = R.vel[D];
     C q2L = L.vel[0] * L.vel[0] + L.vel[1] * L.vel[1] + L.vel[2] * L.vel[2];
     C q2R = R.vel[0] * R.vel[0] + R.vel[1] * R.vel[1] + R.vel[2] * R.vel[2];
-    C cf = (C)0.5 * (sound_speed(L.p, rL) + sound_speed(R.p, rR));
-    C icf = (C)1.0 / cf;
+    C cf = (C)0.5 * (sound_speed<M>(L.p, rL) + sound_speed<M>(R.p, rR));
+    C icf = M::rcp(cf);
     C mL = vnL * icf, mR = vnR * icf;
-    C qbar = sqrt((C)0.5 * (q2L + q2R));
+    C qbar = M::sqrt((C)0.5 * (q2L + q2R));
     C mtil = cmin((C)1.0, icf * qbar);
     C chi = ((C)1.0 - mtil) * ((C)1.0 - mtil);
     C g = -cmax(cmin(mL, (C)0.0), (C)-1.0) * cmin(cmax(mR, (C)0.0), (C)1.0);
-    C vbar = (rL * fabs(vnL) + rR * fabs(vnR)) / (rL + rR);
+    C vbar = M::div(rL * fabs(vnL) + rR * fabs(vnR), rL + rR);
     C vbL = ((C)1.0 - g) * vbar + g * fabs(vnL);
     C vbR = ((C)1.0 - g) * vbar + g * fabs(vnR);
     C mdot = (C)0.5 * (rL * (vnL + vbL) + rR * (vnR - vbR) - (chi * icf) * (R.p - L.p));
@@ -234,14 +291,14 @@ __device__ __forceinline__ void slau2(const FaceState<C>& L, const FaceState<C>&
     f[4] = mdot * ((W.q[4] + W.p) * W.ir);
 }
 
-template <int FLUX, int D, class C>
+template <class M, int FLUX, int D, class C>
 __device__ __forceinline__ void interface_flux(const FaceState<C>& L, const FaceState<C>& R, C* f) {
     if constexpr (FLUX == kSlau2)
-        slau2<D>(L, R, f);
+        slau2<M, D>(L, R, f);
     else if constexpr (FLUX == kAusmPlus)
-        ausm_plus<D>(L, R, f);
+        ausm_plus<M, D>(L, R, f);
     else
-        rusanov<D>(L, R, f);
+        rusanov<M, D>(L, R, f);
 }
 
 }  // namespace od

@@ -10,22 +10,26 @@
 // owns the d-line through face point l (l = j+4k for x, i+4k for y, i+4j for
 // z, the reference's face-point numbering), so 1-D operators act on four
 // registers:
-//   P1  the element state (x-lines, 128-bit loads) -> registers + smem
+//   P1  the element state (x-lines, 128-bit loads) -> smem
 //   P2-4 per direction: own and neighbour face values (BR1 common solution,
 //        slip-wall mirror rhs.cu:111-114), corrected gradient along the line
 //        (rhs.cu:373-461), interface flux F_I and own Euler flux at the two
 //        faces of the line -> j = F_I - Fe_own (slip wall: [0,0,p_w,0,0] - Fe)
-//   P5-6 y / z faces: gradient at the face (11 components), own viscous
+//   P5  x / y / z faces: gradient at the face (11 components), own viscous
 //        flux Fv; j += 1/2 Fv_own; Fv_own -> face buffer for the neighbour
-//   P7  x-threads: pointwise Euler - viscous fluxes of their 4 points
-//        (rhs.cu:229-266), x-divergence in registers, x-face viscous flux
-//   P8-9 y / z divergence along the lines
-//   P10 x-threads: RHS = -div + forcing (rhs.cu:505-509), lifting
+//   P6  x-threads: pointwise Euler - viscous fluxes of their 4 points
+//        (rhs.cu:229-266) -> smem
+//   P7  divergence along x, y, z lines
+//   P8  x-threads: RHS = -div + forcing (rhs.cu:505-509), lifting
 //        -(j_L g_L' + j_R g_R') jac (rk.cu:12-25), RK combination
 //        a*u0 + b*u + c*(RHS + lift) (rk.cu:27-83), 128-bit stores.
 //   The face correction of the reference, j = F_I - 1/2(Fv_L + Fv_R) -
 //   (Fe_own - Fv_own), is complete here except for -1/2 Fv_nbr.
 // Phase B — adds c * lift(-1/2 Fv_nbr) over the element's non-wall faces.
+// With an f32 state phase A stores the unrounded RHS instead of the new state
+// and phase B performs the RK combination, so the state is rounded once per
+// stage: phase B's increments are often below half an f32 ulp of E and rho*u,
+// and rounding the state before adding them would drop them systematically.
 // Only the neighbour's viscous face flux depends on the neighbour's
 // gradient (hence on its own neighbours); everything else is element-local
 // given the six neighbours' face values. Phase B is skipped when mu == 0.
@@ -164,9 +168,9 @@ __device__ __forceinline__ constexpr bool grad_used(int c) {
 // Shared-memory slot of one element in phase A.
 template <class P, class C>
 struct alignas(16) SlotA {
-    C g[15][NE];          // gradient; after P7 F_y in rows 0-4, F_z in 5-9; after P8 div_y in 10-14
-    P u[NV][NE];          // state; after P9 div_z (as C)
-    P tr[6][NV][NF];      // own face values [face = 2d + side][var][face pt]
+    C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9, F_x rows 10-14; P7: div_z rows 10-14
+    P u[NV][NE];          // state; P7: div_x (as C)
+    P tr[6][NV][NF];      // own face values [face = 2d + side][var][face pt]; P7: div_y (as C)
     C j[6][NV][NF];       // face corrections without -1/2 Fv_nbr
 };
 
@@ -174,7 +178,7 @@ template <class S, class P, class C>
 struct StageAParams {
     const S* u_in;
     const S* u0;
-    S* u_out;
+    S* u_out;       // new state, or the RHS when phase B performs the RK combination
     C* fv;          // [elem][face 6][var 4][face pt 16]: own viscous face flux, components 1..4
     Mesh m;
     Tab<P> tp;
@@ -187,9 +191,10 @@ struct StageAParams {
 
 // Interface-flux part of the face correction at one face point, side `side`
 // of direction D: j = F_I - Fe_own, or the slip-wall flux minus Fe_own.
-template <int FLUX, int D, class P, class C>
+template <class M, int FLUX, int D, class P, class C>
 __device__ __forceinline__ void inviscid_face(const P* own, const P* nbr, int side, bool wall, C* j) {
-    FaceState<C> so = make_face_state<C, P>(own);
+    C praw;
+    FaceState<C> so = make_face_state<M, C, P>(own, praw);
     C fe[NV];
     euler_flux<D>(so, fe);
     if (wall) {
@@ -200,18 +205,18 @@ __device__ __forceinline__ void inviscid_face(const P* own, const P* nbr, int si
         j[2] = pw - fe[2];
         return;
     }
-    FaceState<C> sn = make_face_state<C, P>(nbr);
+    FaceState<C> sn = make_face_state<M, C, P>(nbr, praw);
     C fi[NV];
     if (side)
-        interface_flux<FLUX, D>(so, sn, fi);
+        interface_flux<M, FLUX, D>(so, sn, fi);
     else
-        interface_flux<FLUX, D>(sn, so, fi);
+        interface_flux<M, FLUX, D>(sn, so, fi);
 #pragma unroll
     for (int v = 0; v < NV; ++v) j[v] = fi[v] - fe[v];
 }
 
 // P2-P4: one direction of the gradient / face-value pass for line l.
-template <int FLUX, int D, class S, class P, class C>
+template <class M, int FLUX, int D, class S, class P, class C>
 __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, int l,
                                           const long long nb0, const long long nb1, const P (*qreg)[4]) {
     const Mesh& m = A.m;
@@ -291,8 +296,8 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
     }
     // interface fluxes at the two faces of this line
     C j0[NV], j1[NV];
-    inviscid_face<FLUX, D, P, C>(oL, nL, 0, nb0 < 0, j0);
-    inviscid_face<FLUX, D, P, C>(oR, nR, 1, nb1 < 0, j1);
+    inviscid_face<M, FLUX, D, P, C>(oL, nL, 0, nb0 < 0, j0);
+    inviscid_face<M, FLUX, D, P, C>(oR, nR, 1, nb1 < 0, j1);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         sm.j[2 * D][v][l] = j0[v];
@@ -302,15 +307,15 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
 
 // Viscous part at one face point: j += 1/2 Fv_own; Fv_own (components 1..4)
 // to the face buffer for the neighbour's phase B.
-template <int D, class S, class P, class C>
+template <class M, int D, class S, class P, class C>
 __device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
                                              int side, const C* gt, bool live) {
     const int f = 2 * D + side;
     P qp[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) qp[v] = sm.tr[f][v][l];
-    FaceState<C> s = make_face_state<C, P>(qp);
-    const C praw = (C)raw_pressure<P>(qp[0], qp[1], qp[2], qp[3], qp[4]);
+    C praw;
+    FaceState<C> s = make_face_state<M, C, P>(qp, praw);
     C fv[NV];
     viscous_flux<D>(s, praw, gt, A.mu, fv);
 #pragma unroll
@@ -322,8 +327,8 @@ __device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, Slo
     }
 }
 
-// P5 / P6: face gradient along the y or z line of thread l, both faces.
-template <int D, class S, class P, class C>
+// P5: face gradient along the D-line of thread l, viscous flux at both faces.
+template <class M, int D, class S, class P, class C>
 __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
                                                bool wall0, bool wall1, bool live) {
     C gL[15], gR[15];
@@ -335,34 +340,49 @@ __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, S
             continue;
         }
         C w[4];
+        if constexpr (D == 0) {
+            ld4s(&sm.g[c][4 * l], w);
+        } else {
 #pragma unroll
-        for (int mm = 0; mm < 4; ++mm) w[mm] = sm.g[c][line_pt<D>(l, mm)];
+            for (int mm = 0; mm < 4; ++mm) w[mm] = sm.g[c][line_pt<D>(l, mm)];
+        }
         gL[c] = trace4(w, A.tc.eL);
         gR[c] = trace4(w, A.tc.eR);
     }
-    if (!wall0) viscous_face<D>(A, sm, e, l, 0, gL, live);
-    if (!wall1) viscous_face<D>(A, sm, e, l, 1, gR, live);
+    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, gL, live);
+    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, gR, live);
 }
 
-// P8 / P9: divergence of F_D along the line of thread l.
+// P7: divergence of F_D along the line of thread l (times the Jacobian).
 template <int D, class C>
-__device__ __forceinline__ void div_pass(const C (*F)[NE], C* out, int l, const C* Dm, C jac) {
+__device__ __forceinline__ void div_pass(const C* F, C* out, int l, const C* Dm, C jac) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C w[4];
+        if constexpr (D == 0) {
+            ld4s(F + v * NE + 4 * l, w);
+        } else {
 #pragma unroll
-        for (int mm = 0; mm < 4; ++mm) w[mm] = F[v][line_pt<D>(l, mm)];
+            for (int mm = 0; mm < 4; ++mm) w[mm] = F[v * NE + line_pt<D>(l, mm)];
+        }
+        C r[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             C df = (C)0;
 #pragma unroll
             for (int mm = 0; mm < 4; ++mm) df = fma(Dm[a * 4 + mm], w[mm], df);
-            out[v * NE + line_pt<D>(l, a)] = df * jac;
+            r[a] = df * jac;
+        }
+        if constexpr (D == 0) {
+            st4s(out + v * NE + 4 * l, r);
+        } else {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) out[v * NE + line_pt<D>(l, a)] = r[a];
         }
     }
 }
 
-template <class S, class P, class C, int FLUX, int EPB>
+template <class S, class P, class C, class M, int FLUX, int EPB>
 __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S, P, C> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int l = threadIdx.x & (LPE - 1);
@@ -375,103 +395,93 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
     const int ex = (int)(ec % m.nx);
     const int ey = (int)((ec / m.nx) % m.ny);
     const int ez = (int)(ec / ((long long)m.nx * m.ny));
-
-    // ---- P1: the element's x-lines (kept in registers for P2, P7, P10)
-    P ux[NV][4];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        if (live) {
-            ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, ux[v]);
-        } else {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) ux[v][a] = (P)1.0;
-        }
-        st4s(&sm.u[v][4 * l], ux[v]);
-    }
     const long long nxm = neighbour(m, ex, ey, ez, 0, 0), nxp = neighbour(m, ex, ey, ez, 0, 1);
     const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
     const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
-    __syncthreads();
 
-    // ---- P2-P4: face values, gradient, interface fluxes per direction
-    line_pass<FLUX, 0>(A, sm, l, nxm, nxp, ux);
-    line_pass<FLUX, 1>(A, sm, l, nym, nyp, ux);
-    line_pass<FLUX, 2>(A, sm, l, nzm, nzp, ux);
-    __syncthreads();
-
-    // ---- P5-P6: viscous face fluxes of the y and z faces
-    face_grad_pass<1>(A, sm, ec, l, nym < 0, nyp < 0, live);
-    face_grad_pass<2>(A, sm, ec, l, false, false, live);
-    __syncthreads();
-
-    // ---- P7: pointwise fluxes of the x-line, x-divergence, x-face viscous flux
-    C divx[NV][4];
-    C gxL[15], gxR[15];
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-#pragma unroll
-        for (int a = 0; a < 4; ++a) divx[v][a] = (C)0;
-#pragma unroll
-    for (int c = 0; c < 15; ++c) {
-        gxL[c] = (C)0;
-        gxR[c] = (C)0;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int p = 4 * l + i;
-        C g[15];
-#pragma unroll
-        for (int c = 0; c < 15; ++c) g[c] = sm.g[c][p];
-#pragma unroll
-        for (int c = 0; c < 15; ++c) {
-            if (!grad_used<0>(c)) continue;
-            gxL[c] = i == 0 ? g[c] * A.tc.eL[0] : fma(g[c], A.tc.eL[i], gxL[c]);
-            gxR[c] = i == 0 ? g[c] * A.tc.eR[0] : fma(g[c], A.tc.eR[i], gxR[c]);
-        }
-        P qp[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) qp[v] = ux[v][i];
-        FaceState<C> s = make_face_state<C, P>(qp);
-        const C praw = (C)raw_pressure<P>(qp[0], qp[1], qp[2], qp[3], qp[4]);
-        C F[3][NV];
-        volume_fluxes<C>(s, praw, g, A.mu, F);
+    // ---- P1-P2: the element's x-lines, x pass from registers
+    {
+        P ux[NV][4];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
+            if (live) {
+                ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, ux[v]);
+            } else {
 #pragma unroll
-            for (int a = 0; a < 4; ++a) divx[v][a] = fma(A.tc.D[a * 4 + i], F[0][v], divx[v][a]);
-            sm.g[v][p] = F[1][v];
-            sm.g[5 + v][p] = F[2][v];
+                for (int a = 0; a < 4; ++a) ux[v][a] = (P)1.0;
+            }
+            st4s(&sm.u[v][4 * l], ux[v]);
+        }
+        line_pass<M, FLUX, 0>(A, sm, l, nxm, nxp, ux);
+    }
+    __syncthreads();
+    // ---- P3-P4: y and z passes from smem
+    line_pass<M, FLUX, 1>(A, sm, l, nym, nyp, (const P(*)[4]) nullptr);
+    line_pass<M, FLUX, 2>(A, sm, l, nzm, nzp, (const P(*)[4]) nullptr);
+    __syncthreads();
+
+    // ---- P5: viscous face fluxes of all six faces
+    face_grad_pass<M, 0>(A, sm, ec, l, false, false, live);
+    face_grad_pass<M, 1>(A, sm, ec, l, nym < 0, nyp < 0, live);
+    face_grad_pass<M, 2>(A, sm, ec, l, false, false, live);
+    __syncthreads();
+
+    // ---- P6: pointwise fluxes of the x-line's points -> smem (own points only)
+    {
+        P qx[NV][4];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) ld4s(&sm.u[v][4 * l], qx[v]);
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int p = 4 * l + i;
+            C g[15];
+#pragma unroll
+            for (int c = 0; c < 15; ++c) g[c] = sm.g[c][p];
+            P qp[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) qp[v] = i == 0 ? qx[v][0] : i == 1 ? qx[v][1] : i == 2 ? qx[v][2] : qx[v][3];
+            C praw;
+            FaceState<C> s = make_face_state<M, C, P>(qp, praw);
+            C F[3][NV];
+            volume_fluxes<C>(s, praw, g, A.mu, F);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                sm.g[v][p] = F[1][v];
+                sm.g[5 + v][p] = F[2][v];
+                sm.g[10 + v][p] = F[0][v];
+            }
         }
     }
-    viscous_face<0>(A, sm, ec, l, 0, gxL, live);
-    viscous_face<0>(A, sm, ec, l, 1, gxR, live);
     __syncthreads();
 
-    // ---- P8-P9: y and z divergence along the lines
-    C* divz = reinterpret_cast<C*>(&sm.u[0][0]);
-    div_pass<1, C>(sm.g, &sm.g[10][0], l, A.tc.D, A.jac[1]);
-    div_pass<2, C>(&sm.g[5], divz, l, A.tc.D, A.jac[2]);
+    // ---- P7: divergences (x -> u region, y -> tr region, then z -> rows 10-14)
+    C* divx = reinterpret_cast<C*>(&sm.u[0][0]);
+    C* divy = reinterpret_cast<C*>(&sm.tr[0][0][0]);
+    div_pass<0, C>(&sm.g[10][0], divx, l, A.tc.D, A.jac[0]);
+    div_pass<1, C>(&sm.g[0][0], divy, l, A.tc.D, A.jac[1]);
+    __syncthreads();
+    div_pass<2, C>(&sm.g[5][0], &sm.g[10][0], l, A.tc.D, A.jac[2]);
     __syncthreads();
 
-    // ---- P10: RHS, lifting, RK combination
+    // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
     if (!live) return;
     const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
+    const bool defer = (A.flags & kDeferRK) != 0;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        C dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
-        ld4s(&sm.g[10 + v][4 * l], dy);
-        ld4s(&divz[v * NE + 4 * l], dz);
+        C dx[4], dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
+        ld4s(&divx[v * NE + 4 * l], dx);
+        ld4s(&divy[v * NE + 4 * l], dy);
+        ld4s(&sm.g[10 + v][4 * l], dz);
         ld4s(&sm.j[2][v][4 * lk], jy0);
         ld4s(&sm.j[3][v][4 * lk], jy1);
         ld4s(&sm.j[4][v][4 * lj], jz0);
         ld4s(&sm.j[5][v][4 * lj], jz1);
         const C jx0 = sm.j[0][v][l], jx1 = sm.j[1][v][l];
-        P u0v[4];
-        if (A.flags & kHasU0) ldg4<S, P>(A.u0 + v * m.npts + ec * NE + 4 * l, u0v);
-        P out[4];
+        C rt[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            C rvol = -((divx[v][i] * A.jac[0] + dy[i]) + dz[i]);
+            C rvol = -((dx[i] + dy[i]) + dz[i]);
             if (v == 1) rvol += A.forcing;
             if constexpr (sizeof(C) == 8) {
                 if (A.flags & kRoundRhs) rvol = (C)(float)rvol;
@@ -479,26 +489,42 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
             const C cx = -(jx0 * A.tc.gL[i] * A.jac[0]) - (jx1 * A.tc.gR[i] * A.jac[0]);
             const C cy = -(jy0[i] * A.tc.gL[lj] * A.jac[1]) - (jy1[i] * A.tc.gR[lj] * A.jac[1]);
             const C cz = -(jz0[i] * A.tc.gL[lk] * A.jac[2]) - (jz1[i] * A.tc.gR[lk] * A.jac[2]);
-            const C rtot = rvol + (cx + cy + cz);
-            P o = A.rb * ux[v][i] + A.rc * (P)rtot;
-            if (A.flags & kHasU0) o = A.ra * u0v[i] + A.rb * ux[v][i] + A.rc * (P)rtot;
+            rt[i] = rvol + (cx + cy + cz);
+        }
+        S* dst = A.u_out + v * m.npts + ec * NE + 4 * l;
+        if (defer) {
+            stg4<S, C>(dst, rt);
+            continue;
+        }
+        P un[4], u0v[4], out[4];
+        ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, un);
+        if (A.flags & kHasU0) ldc4<S, P>(A.u0 + v * m.npts + ec * NE + 4 * l, u0v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            P o = A.rb * un[i] + A.rc * (P)rt[i];
+            if (A.flags & kHasU0) o = A.ra * u0v[i] + A.rb * un[i] + A.rc * (P)rt[i];
             out[i] = o;
         }
-        stg4<S, P>(A.u_out + v * m.npts + ec * NE + 4 * l, out);
+        stg4<S, P>(dst, out);
     }
 }
 
 template <class S, class P, class C>
 struct StageBParams {
     S* u_out;
+    const S* rhs;   // deferred RK: phase A's RHS
+    const S* u_in;
+    const S* u0;
     const C* fv;
     Mesh m;
     Tab<C> tc;
     C jac[3];
-    P rc;
+    P ra, rb, rc;
+    int flags;
 };
 
-// Phase B: u_out += rc * lift(-1/2 Fv_nbr) over the element's non-wall faces;
+// Phase B: rc * lift(-1/2 Fv_nbr) over the element's non-wall faces, added to
+// the new state, or (deferred RK) u_out = ra*u0 + rb*u_in + rc*(RHS + lift).
 // 16 threads per element, each the x-line l = j + 4k (128-bit accesses).
 template <class S, class P, class C, int EPB>
 __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
@@ -514,6 +540,23 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
     const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
     const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
     const C hx = (C)0.5 * B.jac[0], hy = (C)0.5 * B.jac[1], hz = (C)0.5 * B.jac[2];
+    const bool defer = (B.flags & kDeferRK) != 0;
+    if (defer) {
+        // density has no viscous term: only the RK combination
+        const long long off = e * NE + 4 * l;
+        C r[4];
+        P un[4], u0v[4], out[4];
+        ldg4<S, C>(B.rhs + off, r);
+        ldg4<S, P>(B.u_in + off, un);
+        if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, u0v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            P o = B.rb * un[i] + B.rc * (P)r[i];
+            if (B.flags & kHasU0) o = B.ra * u0v[i] + B.rb * un[i] + B.rc * (P)r[i];
+            out[i] = o;
+        }
+        stg4<S, P>(B.u_out + off, out);
+    }
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         C acc[4] = {(C)0, (C)0, (C)0, (C)0};
@@ -546,12 +589,28 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
 #pragma unroll
             for (int i = 0; i < 4; ++i) acc[i] = fma(c0, w0[i], fma(c1, w1[i], acc[i]));
         }
-        S* p = B.u_out + (v + 1) * m.npts + e * NE + 4 * l;
-        P cur[4];
-        ldc4<S, P>(p, cur);
+        const long long off = (v + 1) * m.npts + e * NE + 4 * l;
+        P out[4];
+        if (defer) {
+            C r[4];
+            P un[4], u0v[4];
+            ldg4<S, C>(B.rhs + off, r);
+            ldg4<S, P>(B.u_in + off, un);
+            if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, u0v);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) cur[i] = cur[i] + B.rc * (P)acc[i];
-        stg4<S, P>(p, cur);
+            for (int i = 0; i < 4; ++i) {
+                const C rt = r[i] + acc[i];
+                P o = B.rb * un[i] + B.rc * (P)rt;
+                if (B.flags & kHasU0) o = B.ra * u0v[i] + B.rb * un[i] + B.rc * (P)rt;
+                out[i] = o;
+            }
+        } else {
+            P cur[4];
+            ldc4<S, P>(B.u_out + off, cur);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) out[i] = cur[i] + B.rc * (P)acc[i];
+        }
+        stg4<S, P>(B.u_out + off, out);
     }
 }
 
