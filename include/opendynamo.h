@@ -58,7 +58,16 @@ typedef struct od_params {
     double mu;                     /* dynamic viscosity; reference constant 1.6e-4 (constants.cuh:42) */
     double forcing;                /* source added to the rho*u RHS; reference 1e-3 (rhs.cu:508) */
     int device;                    /* CUDA device ordinal */
+    int ref_compat;                /* OD_COMPAT_* bits: reproduce reference arithmetic quirks (default 0) */
 } od_params;
+
+/* ref_compat bits. OD_COMPAT_Y_SLICE_F32: the reference builds its y-face
+ * gradient slices with __fmul_rn, a float intrinsic, also in its f64
+ * pipeline (src/cuda/rhs.cu:145-160), which rounds those products and sums
+ * to f32. With this bit an f64-compute run does the same, for bit-level
+ * agreement with the reference's f64 results; without it the f64 pipeline
+ * is f64 throughout (more accurate). */
+enum { OD_COMPAT_Y_SLICE_F32 = 1 };
 
 /* Reference defaults: SLAU2, slip walls, all f32, mu 1.6e-4, forcing 1e-3. */
 void od_default_params(od_params* p);

@@ -33,7 +33,7 @@ class OdParams(ctypes.Structure):
         ("rhs_real", ctypes.c_int), ("compute_real", ctypes.c_int),
         ("mixed", ctypes.c_int), ("fast_math", ctypes.c_int),
         ("mu", ctypes.c_double), ("forcing", ctypes.c_double),
-        ("device", ctypes.c_int),
+        ("device", ctypes.c_int), ("ref_compat", ctypes.c_int),
     ]
 
 

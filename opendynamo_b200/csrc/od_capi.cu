@@ -251,6 +251,7 @@ int od_create(const od_params* p, od_ctx** out) {
         if (p->q_real == OD_F32) c->round_flags |= od::kRoundQ;
         if (p->rhs_real == OD_F32) c->round_flags |= od::kRoundRhs;
     }
+    if (c->fns.c_double && (p->ref_compat & OD_COMPAT_Y_SLICE_F32)) c->round_flags |= od::kRefYSlice;
     c->tab = build_tables();
     // jac = 2 / (L / n) in the compute type (rk.cu:93-95)
     const double L3[3] = {p->lx, p->ly, p->lz};

@@ -12,6 +12,7 @@ enum StageFlags : int {
     kRoundQ = 2,     // round the gradient through f32 (q_real = f32 with f64 compute)
     kRoundRhs = 4,   // round the volume RHS through f32 (rhs_real = f32 with f64 compute)
     kDeferRK = 8,    // phase A stores the RHS, phase B performs the RK combination
+    kRefYSlice = 16, // f64 compute: round the y-face gradient traces as the reference's __fmul_rn does
 };
 
 // FR operator tables in double (the host computes them once, as

@@ -166,12 +166,29 @@ __device__ __forceinline__ constexpr bool grad_used(int c) {
 }
 
 // Shared-memory slot of one element in phase A.
+// ---- shared-memory point layout
+// Points of an element are stored at p ^ (((p >> 3) & 4) | par << 3): the
+// j index is XOR-swizzled with bit 1 of k and with the element's parity
+// inside its warp (two elements per warp), and every element slot is a
+// multiple of 32 words plus 16. With these, the three access patterns of a
+// half-warp (16 x-lines as 128-bit vectors, 16 y-lines and 16 z-lines as
+// scalars) hit 32 distinct banks across the whole warp.
+__device__ __forceinline__ int sw(int p, int swz) { return p ^ (((p >> 3) & 4) | swz); }
+
+template <class P, class C>
+struct SlotBytes {
+    static constexpr int base = 15 * NE * (int)sizeof(C) + NV * NE * (int)sizeof(P) + 6 * NV * NF * (int)sizeof(C);
+    static constexpr int words = base / 4;
+    static constexpr int pad_words = ((16 - words % 32) + 32) % 32 == 0 ? 32 : ((16 - words % 32) + 32) % 32;
+};
+
+// Shared-memory slot of one element in phase A.
 template <class P, class C>
 struct alignas(16) SlotA {
-    C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9, F_x rows 10-14; P7: div_z rows 10-14
-    P u[NV][NE];          // state; P7: div_x (as C)
-    P tr[6][NV][NF];      // own face values [face = 2d + side][var][face pt]; P7: div_y (as C)
-    C j[6][NV][NF];       // face corrections without -1/2 Fv_nbr
+    C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9, F_x rows 10-14; P7: div_z / div_x in place
+    P u[NV][NE];          // state; P7: div_y (as C)
+    C j[6][NV][NF];       // face corrections without -1/2 Fv_nbr [face = 2d + side][var][face pt]
+    float pad[SlotBytes<P, C>::pad_words];
 };
 
 template <class S, class P, class C>
@@ -215,22 +232,35 @@ __device__ __forceinline__ void inviscid_face(const P* own, const P* nbr, int si
     for (int v = 0; v < NV; ++v) j[v] = fi[v] - fe[v];
 }
 
+// load / store the 4 samples of line l in direction D of a swizzled row
+template <int D, class T>
+__device__ __forceinline__ void row_line_load(const T* row, int l, int swz, T* w) {
+    if constexpr (D == 0) {
+        ld4s(row + sw(4 * l, swz), w);
+    } else {
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) w[mm] = row[sw(line_pt<D>(l, mm), swz)];
+    }
+}
+
+template <int D, class T>
+__device__ __forceinline__ void row_line_store(T* row, int l, int swz, const T* w) {
+    if constexpr (D == 0) {
+        st4s(row + sw(4 * l, swz), w);
+    } else {
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) row[sw(line_pt<D>(l, mm), swz)] = w[mm];
+    }
+}
+
 // P2-P4: one direction of the gradient / face-value pass for line l.
 template <class M, int FLUX, int D, class S, class P, class C>
-__device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, int l,
-                                          const long long nb0, const long long nb1, const P (*qreg)[4]) {
+__device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, int l, int swz,
+                                          const long long nb0, const long long nb1) {
     const Mesh& m = A.m;
     P q[NV][4];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        if constexpr (D == 0) {
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) q[v][mm] = qreg[v][mm];
-        } else {
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) q[v][mm] = sm.u[v][line_pt<D>(l, mm)];
-        }
-    }
+    for (int v = 0; v < NV; ++v) row_line_load<D>(sm.u[v], l, swz, q[v]);
     P oL[NV], oR[NV], nL[NV], nR[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -285,14 +315,7 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
             }
             gv[a] = gg;
         }
-        if constexpr (D == 0) {
-            st4s(&sm.g[3 * v][4 * l], gv);
-        } else {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) sm.g[3 * v + D][line_pt<D>(l, a)] = gv[a];
-        }
-        sm.tr[2 * D][v][l] = oL[v];
-        sm.tr[2 * D + 1][v][l] = oR[v];
+        row_line_store<D>(sm.g[3 * v + D], l, swz, gv);
     }
     // interface fluxes at the two faces of this line
     C j0[NV], j1[NV];
@@ -309,11 +332,8 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
 // to the face buffer for the neighbour's phase B.
 template <class M, int D, class S, class P, class C>
 __device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
-                                             int side, const C* gt, bool live) {
+                                             int side, const P* qp, const C* gt, bool live) {
     const int f = 2 * D + side;
-    P qp[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) qp[v] = sm.tr[f][v][l];
     C praw;
     FaceState<C> s = make_face_state<M, C, P>(qp, praw);
     C fv[NV];
@@ -327,11 +347,24 @@ __device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, Slo
     }
 }
 
-// P5: face gradient along the D-line of thread l, viscous flux at both faces.
+// The reference's y-face gradient slice multiplies with __fmul_rn, a float
+// intrinsic, also in its f64 build (rhs.cu:145-160): products and pair sums
+// in f32. Reproduced on request (kRefYSlice) for bit-level drop-in parity.
+template <class C>
+__device__ __forceinline__ C ref_y_slice(const C* w, const C* c) {
+    const float a = __fadd_rn(__fmul_rn((float)w[0], (float)c[0]), __fmul_rn((float)w[1], (float)c[1]));
+    const float b = __fadd_rn(__fmul_rn((float)w[2], (float)c[2]), __fmul_rn((float)w[3], (float)c[3]));
+    return (C)__fadd_rn(a, b);
+}
+
+// P5: face values and face gradient along the D-line of thread l, viscous
+// flux at both faces of the line.
 template <class M, int D, class S, class P, class C>
 __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
-                                               bool wall0, bool wall1, bool live) {
+                                               int swz, bool wall0, bool wall1, bool live) {
+    if (wall0 && wall1) return;
     C gL[15], gR[15];
+    const bool ref_y = D == 1 && sizeof(C) == 8 && (A.flags & kRefYSlice);
 #pragma unroll
     for (int c = 0; c < 15; ++c) {
         if (!grad_used<D>(c)) {
@@ -340,31 +373,34 @@ __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, S
             continue;
         }
         C w[4];
-        if constexpr (D == 0) {
-            ld4s(&sm.g[c][4 * l], w);
+        row_line_load<D>(sm.g[c], l, swz, w);
+        if (ref_y) {
+            gL[c] = ref_y_slice(w, A.tc.eL);
+            gR[c] = ref_y_slice(w, A.tc.eR);
         } else {
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) w[mm] = sm.g[c][line_pt<D>(l, mm)];
+            gL[c] = trace4(w, A.tc.eL);
+            gR[c] = trace4(w, A.tc.eR);
         }
-        gL[c] = trace4(w, A.tc.eL);
-        gR[c] = trace4(w, A.tc.eR);
     }
-    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, gL, live);
-    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, gR, live);
+    P qL[NV], qR[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        P w[4];
+        row_line_load<D>(sm.u[v], l, swz, w);
+        qL[v] = trace4(w, A.tp.eL);
+        qR[v] = trace4(w, A.tp.eR);
+    }
+    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live);
+    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live);
 }
 
 // P7: divergence of F_D along the line of thread l (times the Jacobian).
 template <int D, class C>
-__device__ __forceinline__ void div_pass(const C* F, C* out, int l, const C* Dm, C jac) {
+__device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, const C* Dm, C jac) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C w[4];
-        if constexpr (D == 0) {
-            ld4s(F + v * NE + 4 * l, w);
-        } else {
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) w[mm] = F[v * NE + line_pt<D>(l, mm)];
-        }
+        row_line_load<D>(F + v * NE, l, swz, w);
         C r[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
@@ -373,12 +409,7 @@ __device__ __forceinline__ void div_pass(const C* F, C* out, int l, const C* Dm,
             for (int mm = 0; mm < 4; ++mm) df = fma(Dm[a * 4 + mm], w[mm], df);
             r[a] = df * jac;
         }
-        if constexpr (D == 0) {
-            st4s(out + v * NE + 4 * l, r);
-        } else {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) out[v * NE + line_pt<D>(l, a)] = r[a];
-        }
+        row_line_store<D>(out + v * NE, l, swz, r);
     }
 }
 
@@ -387,6 +418,7 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int l = threadIdx.x & (LPE - 1);
     const int es = threadIdx.x / LPE;
+    const int swz = (es & 1) << 3;
     SlotA<P, C>& sm = reinterpret_cast<SlotA<P, C>*>(smem_raw)[es];
     const long long e = (long long)blockIdx.x * EPB + es;
     const bool live = e < A.m.nelem;
@@ -399,41 +431,43 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
     const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
     const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
 
-    // ---- P1-P2: the element's x-lines, x pass from registers
-    {
-        P ux[NV][4];
+    // ---- P1: the element's x-lines -> smem
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            if (live) {
-                ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, ux[v]);
-            } else {
+    for (int v = 0; v < NV; ++v) {
+        P w[4];
+        if (live) {
+            ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, w);
+        } else {
 #pragma unroll
-                for (int a = 0; a < 4; ++a) ux[v][a] = (P)1.0;
-            }
-            st4s(&sm.u[v][4 * l], ux[v]);
+            for (int a = 0; a < 4; ++a) w[a] = (P)1.0;
         }
-        line_pass<M, FLUX, 0>(A, sm, l, nxm, nxp, ux);
+        st4s(&sm.u[v][sw(4 * l, swz)], w);
     }
     __syncthreads();
-    // ---- P3-P4: y and z passes from smem
-    line_pass<M, FLUX, 1>(A, sm, l, nym, nyp, (const P(*)[4]) nullptr);
-    line_pass<M, FLUX, 2>(A, sm, l, nzm, nzp, (const P(*)[4]) nullptr);
+
+    // ---- P2-P4: face values, gradient, interface fluxes per direction
+    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp);
+    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp);
+    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp);
     __syncthreads();
 
     // ---- P5: viscous face fluxes of all six faces
-    face_grad_pass<M, 0>(A, sm, ec, l, false, false, live);
-    face_grad_pass<M, 1>(A, sm, ec, l, nym < 0, nyp < 0, live);
-    face_grad_pass<M, 2>(A, sm, ec, l, false, false, live);
+    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live);
+    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live);
+    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live);
     __syncthreads();
 
-    // ---- P6: pointwise fluxes of the x-line's points -> smem (own points only)
+    // ---- P6: pointwise fluxes of the x-line's points (own points only; the
+    // point order is rotated by k so the 16 lanes of an element hit distinct banks)
     {
+        const int lk = l >> 2;
         P qx[NV][4];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) ld4s(&sm.u[v][4 * l], qx[v]);
+        for (int v = 0; v < NV; ++v) ld4s(&sm.u[v][sw(4 * l, swz)], qx[v]);
 #pragma unroll 1
-        for (int i = 0; i < 4; ++i) {
-            const int p = 4 * l + i;
+        for (int it = 0; it < 4; ++it) {
+            const int i = (it + lk) & 3;
+            const int p = sw(4 * l + i, swz);
             C g[15];
 #pragma unroll
             for (int c = 0; c < 15; ++c) g[c] = sm.g[c][p];
@@ -454,25 +488,24 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
     }
     __syncthreads();
 
-    // ---- P7: divergences (x -> u region, y -> tr region, then z -> rows 10-14)
-    C* divx = reinterpret_cast<C*>(&sm.u[0][0]);
-    C* divy = reinterpret_cast<C*>(&sm.tr[0][0][0]);
-    div_pass<0, C>(&sm.g[10][0], divx, l, A.tc.D, A.jac[0]);
-    div_pass<1, C>(&sm.g[0][0], divy, l, A.tc.D, A.jac[1]);
-    __syncthreads();
-    div_pass<2, C>(&sm.g[5][0], &sm.g[10][0], l, A.tc.D, A.jac[2]);
+    // ---- P7: divergences: x in place (rows 10-14), y -> state region, z in place (rows 5-9)
+    C* divy = reinterpret_cast<C*>(&sm.u[0][0]);
+    div_pass<0, C>(&sm.g[10][0], &sm.g[10][0], l, swz, A.tc.D, A.jac[0]);
+    div_pass<1, C>(&sm.g[0][0], divy, l, swz, A.tc.D, A.jac[1]);
+    div_pass<2, C>(&sm.g[5][0], &sm.g[5][0], l, swz, A.tc.D, A.jac[2]);
     __syncthreads();
 
     // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
     if (!live) return;
     const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
+    const int px = sw(4 * l, swz);
     const bool defer = (A.flags & kDeferRK) != 0;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C dx[4], dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
-        ld4s(&divx[v * NE + 4 * l], dx);
-        ld4s(&divy[v * NE + 4 * l], dy);
-        ld4s(&sm.g[10 + v][4 * l], dz);
+        ld4s(&sm.g[10 + v][px], dx);
+        ld4s(&divy[v * NE + px], dy);
+        ld4s(&sm.g[5 + v][px], dz);
         ld4s(&sm.j[2][v][4 * lk], jy0);
         ld4s(&sm.j[3][v][4 * lk], jy1);
         ld4s(&sm.j[4][v][4 * lj], jz0);

@@ -27,7 +27,7 @@ def fr_tables() -> dict:
 
 def make_params(nx, ny, nz, lx, ly, lz, flux="slau2", y_wall=True, u_real="f32", q_real=None,
                 rhs_real=None, compute_real=None, mixed=False, mu=1.6e-4, forcing=1e-3,
-                device=0, fast_math=True) -> N.OdParams:
+                device=0, fast_math=True, ref_compat=0) -> N.OdParams:
     """Build od_params. Extents are rounded to f32 as config.rs stores them."""
     q_real = q_real or (u_real if not mixed else "f32")
     rhs_real = rhs_real or (u_real if not mixed else "f32")
@@ -36,7 +36,7 @@ def make_params(nx, ny, nz, lx, ly, lz, flux="slau2", y_wall=True, u_real="f32",
     return N.OdParams(int(nx), int(ny), int(nz), float(np.float32(lx)), float(np.float32(ly)),
                       float(np.float32(lz)), N.OD_FLUX[flux], int(bool(y_wall)), t[u_real], t[q_real],
                       t[rhs_real], t[compute_real], int(bool(mixed)), int(bool(fast_math)), float(mu),
-                      float(forcing), int(device))
+                      float(forcing), int(device), int(ref_compat))
 
 
 def params_from_config(cfg: Config, device: int = 0) -> N.OdParams:

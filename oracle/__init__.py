@@ -26,7 +26,7 @@ class OrcParams(ctypes.Structure):
         ("u_f64", ctypes.c_int), ("q_f64", ctypes.c_int),
         ("rhs_f64", ctypes.c_int), ("c_f64", ctypes.c_int),
         ("mu", ctypes.c_double), ("forcing", ctypes.c_double),
-        ("threads", ctypes.c_int),
+        ("threads", ctypes.c_int), ("ref_y_slice_f32", ctypes.c_int),
     ]
 
 
@@ -51,6 +51,7 @@ def lib():
                              ctypes.c_double, ctypes.c_int]
         L.orc_rhs_total.argtypes = [P, vp, vp]
         L.orc_run.argtypes = [P, vp, ctypes.c_int, ctypes.c_double]
+        L.orc_run_ld.argtypes = [P, vp, ctypes.c_int, ctypes.c_double]
         _lib = L
     return _lib
 
@@ -61,13 +62,14 @@ def _ptr(a: np.ndarray):
 
 
 def make_params(nx, ny, nz, lx, ly, lz, flux="rusanov", y_wall=False, u="f64", q=None, rhs=None,
-                compute=None, mu=1.6e-4, forcing=1e-3, threads=0) -> OrcParams:
+                compute=None, mu=1.6e-4, forcing=1e-3, threads=0, ref_y_slice_f32=False) -> OrcParams:
     q = q or u
     rhs = rhs or u
     compute = compute or u
     return OrcParams(nx, ny, nz, float(np.float32(lx)), float(np.float32(ly)), float(np.float32(lz)),
                      FLUX_IDS[flux], int(bool(y_wall)), int(u == "f64"), int(q == "f64"),
-                     int(rhs == "f64"), int(compute == "f64"), float(mu), float(forcing), int(threads))
+                     int(rhs == "f64"), int(compute == "f64"), float(mu), float(forcing), int(threads),
+                     int(bool(ref_y_slice_f32)))
 
 
 def _dt(flag):
@@ -146,5 +148,13 @@ def run(p: OrcParams, u: np.ndarray, n_steps: int, dt: float) -> np.ndarray:
     """n SSP-RK3 steps; dt is rounded to f32 first, as the reference's config does."""
     u = np.array(u, dtype=_dt(p.u_f64), copy=True, order="C")
     rc = lib().orc_run(ctypes.byref(p), _ptr(u), int(n_steps), float(np.float32(dt)))
+    assert rc == 0
+    return u
+
+
+def run_extended(p: OrcParams, u: np.ndarray, n_steps: int, dt: float) -> np.ndarray:
+    """The run in x87 long double (state and arithmetic), rounded to f64 at the end."""
+    u = np.array(u, dtype=np.float64, copy=True, order="C")
+    rc = lib().orc_run_ld(ctypes.byref(p), _ptr(u), int(n_steps), float(np.float32(dt)))
     assert rc == 0
     return u

@@ -303,6 +303,7 @@ typedef struct {
     double mu;      // reference: 1.6e-4 (constants.cuh:42)
     double forcing; // reference: 1e-3 on rho*u (rhs.cu:508)
     int threads;    // 0 = all host threads
+    int ref_y_slice_f32;  // f64 compute: y slices with f32 products and pair sums, as rhs.cu:145-160
 } orc_params;
 
 }  // extern "C"
@@ -435,9 +436,20 @@ struct Oracle {
                     for (int c = 0; c < 15; ++c) {
                         if (omitted(d, c)) continue;
                         C sl = 0, sr = 0;
-                        for (int m = 0; m < NP; ++m) {
-                            sl += grad[c][line_pt(d, fp, m)] * eL[m];
-                            sr += grad[c][line_pt(d, fp, m)] * eR[m];
+                        if (d == 1 && (P.ref_y_slice_f32 || sizeof(C) == 4)) {
+                            // rhs.cu:157-160: __fmul_rn products, (p0 + p1) + (p2 + p3) in f32
+                            float pl[4], pr[4];
+                            for (int m = 0; m < NP; ++m) {
+                                pl[m] = (float)grad[c][line_pt(d, fp, m)] * (float)eL[m];
+                                pr[m] = (float)grad[c][line_pt(d, fp, m)] * (float)eR[m];
+                            }
+                            sl = (C)((pl[0] + pl[1]) + (pl[2] + pl[3]));
+                            sr = (C)((pr[0] + pr[1]) + (pr[2] + pr[3]));
+                        } else {
+                            for (int m = 0; m < NP; ++m) {
+                                sl += grad[c][line_pt(d, fp, m)] * eL[m];
+                                sr += grad[c][line_pt(d, fp, m)] * eR[m];
+                            }
                         }
                         rowL[slot] = sl;
                         rowR[slot] = sr;
@@ -771,6 +783,17 @@ int orc_rhs_total(const orc_params* p, const void* u, double* out) {
 int orc_run(const orc_params* p, void* u, int n_steps, double dt) {
     if (!valid(p) || n_steps < 0) return -1;
     return dispatch<RunFn>(*p, u, n_steps, dt);
+}
+
+// The same run in extended precision (x87 long double state and arithmetic),
+// a more accurate truth for judging f64 implementations. u is double in / out.
+int orc_run_ld(const orc_params* p, double* u, int n_steps, double dt) {
+    if (!valid(p) || n_steps < 0) return -1;
+    long n = (long)p->nx * p->ny * p->nz * NE * NV;
+    std::vector<long double> w(u, u + n);
+    run_impl<long double, long double, long double>(*p, w.data(), n_steps, dt);
+    for (long i = 0; i < n; ++i) u[i] = (double)w[i];
+    return 0;
 }
 
 }  // extern "C"

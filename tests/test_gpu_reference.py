@@ -2,7 +2,15 @@
 sources, launched like src/solver.rs) on identical initial states.
 
 Bars (relative L2 per variable after 100 steps): f64 pipeline 1e-10,
-f32 pipeline 1e-5. Also pins the CPU oracle kernel by kernel.
+f32 pipeline 1e-5 (see helpers.assert_f32_parity). Also pins the CPU oracle
+kernel by kernel.
+
+The reference's f64 build is not f64 throughout: its y-face gradient slices
+use the float intrinsic __fmul_rn (rhs.cu:145-160), which puts it ~1e-10
+(relative, on rho*w of the TGV) away from an extended-precision solution.
+f64 comparisons against the reference therefore run this project's kernels
+with OD_COMPAT_Y_SLICE_F32; the default f64 pipeline is checked against the
+extended-precision oracle run instead.
 """
 
 from __future__ import annotations
@@ -36,13 +44,33 @@ def test_tgv_f64_100_steps_vs_reference():
         r.set_state(u)
         r.step(100, dt)
         ref = r.get_state()
-    with Solver(make_params(n, n, n, L, L, L, "rusanov", False, "f64")) as s:
+    with Solver(make_params(n, n, n, L, L, L, "rusanov", False, "f64", ref_compat=1)) as s:
         s.set_state(u)
         s.step(100, dt)
         got = s.get_state()
     err = rel_l2(got, ref)
     assert np.all(err < 1e-10), err
     assert np.all(rel_l2(got - u, ref - u) < 1e-8)
+
+
+@pytest.mark.gpu
+def test_tgv_f64_100_steps_vs_extended_precision():
+    """The default f64 pipeline against the oracle's x87 extended-precision
+    run of config 1: as accurate as the f64 CPU restatement."""
+    n = 8
+    L = 2 * math.pi
+    u = tgv(n)
+    dt = float(np.float32(tgv_dt(n)))
+    op = oracle.make_params(n, n, n, L, L, L, flux="rusanov", y_wall=False, u="f64")
+    truth = oracle.run_extended(op, u, 100, dt)
+    orc = oracle.run(op, u, 100, dt)
+    with Solver(make_params(n, n, n, L, L, L, "rusanov", False, "f64")) as s:
+        s.set_state(u)
+        s.step(100, dt)
+        got = s.get_state()
+    err = rel_l2(got, truth)
+    assert np.all(err < 1e-10), err
+    assert np.all(err <= np.maximum(4 * rel_l2(orc, truth), 1e-14)), (err, rel_l2(orc, truth))
 
 
 @pytest.mark.gpu
@@ -82,7 +110,7 @@ def test_steps_vs_reference(prec, wall, flux):
         r.set_state(u)
         r.step(20, dt)
         ref = r.get_state()
-    with Solver(make_params(*mesh, *BOX, flux, wall, prec)) as s:
+    with Solver(make_params(*mesh, *BOX, flux, wall, prec, ref_compat=1)) as s:
         s.set_state(u)
         s.step(20, float(np.float32(dt)))
         got = s.get_state()
@@ -104,7 +132,7 @@ def test_oracle_kernels_vs_reference_f64(flux, wall):
     """Kernel by kernel: volume RHS + slices, face corrections, RK stage."""
     mesh = (3, 4, 2)
     u = random_smooth(*mesh, seed=7)
-    op = oracle.make_params(*mesh, *BOX, flux=flux, y_wall=wall, u="f64")
+    op = oracle.make_params(*mesh, *BOX, flux=flux, y_wall=wall, u="f64", ref_y_slice_f32=True)
     with _ref()(*mesh, *BOX, flux, wall, "f64") as r:
         r.set_state(u)
         r.rhs_stage()
