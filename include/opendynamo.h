@@ -38,7 +38,8 @@ enum {
     OD_ERR_CUDA = -2,   /* a CUDA call failed (see od_last_error) */
     OD_ERR_SIZE = -3,   /* buffer size does not match the mesh */
     OD_ERR_STATE = -4,  /* call out of order (e.g. no state set) */
-    OD_ERR_IO = -5      /* state-file read/write failure */
+    OD_ERR_IO = -5,     /* state-file read/write failure */
+    OD_ERR_SCRATCH = -6 /* od_rhs_noalloc: the mesh needs more than OD_NOALLOC_SCRATCH_BYTES */
 };
 
 typedef struct od_ctx od_ctx;
@@ -126,6 +127,28 @@ int od_set_launch_shape(od_ctx* ctx, int elems_per_block_a, int elems_per_block_
  * last reset (synchronizes the stream). */
 int od_set_timing(od_ctx* ctx, int enabled);
 int od_timing(od_ctx* ctx, double* ms_phase_a, double* ms_phase_b, long long* n_stages);
+
+/* Full right-hand side of a device-resident state without allocating
+ * anything: no context, no cudaMalloc / cudaFree, no allocating library call.
+ * No counterpart in the reference (its host allocates every buffer up front);
+ * it serves callers that cannot allocate device memory when they need an RHS,
+ * e.g. code inside another framework's step callback that owns the device
+ * memory, or fixed-footprint loops. The caller passes the state (d_state, 5
+ * planes of u_real) and the output (d_rhs, same size, not aliasing d_state) in
+ * device memory; the result equals od_rhs on a context with the same params.
+ * The kernels' only scratch, the per-face viscous fluxes, lives in one static
+ * device array of OD_NOALLOC_SCRATCH_BYTES per GPU (held until exit), which
+ * limits the mesh to OD_NOALLOC_SCRATCH_BYTES / (384 * sizeof(compute type))
+ * elements (10922 in f32 compute, 5461 in f64); larger meshes return
+ * OD_ERR_SCRATCH. All calls share the array: calls whose kernels overlap on
+ * the GPU race, so order them on one stream. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) and sets the kernels'
+ * shared-memory limits; make it before any stream capture. Runs on
+ * params->device (the caller's current device is restored) and enqueues on
+ * `stream` (cudaStream_t, null = legacy default stream); returns before the
+ * kernels finish. */
+#define OD_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int od_rhs_noalloc(const od_params* params, const void* d_state, void* d_rhs, size_t bytes, void* stream);
 
 /* Message of the last failure on this context ("" if none). */
 const char* od_last_error(const od_ctx* ctx);

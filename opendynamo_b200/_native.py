@@ -14,13 +14,15 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libo
 OD_FLUX = {"slau2": 0, "ausm+": 1, "rusanov": 2}
 OD_F32, OD_F64 = 0, 1
 
-ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "size mismatch", -4: "call out of order", -5: "I/O error"}
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "size mismatch", -4: "call out of order", -5: "I/O error",
+          -6: "mesh exceeds the no-alloc scratch"}
 
 # every symbol include/opendynamo.h declares
 EXPORTS = (
     "od_default_params", "od_create", "od_destroy", "od_state_bytes", "od_set_state", "od_get_state",
     "od_set_state_device", "od_get_state_device", "od_step", "od_rhs", "od_sync", "od_stream",
     "od_launches_per_step", "od_set_launch_shape", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
+    "od_rhs_noalloc",
 )
 
 
@@ -73,6 +75,7 @@ def lib() -> ctypes.CDLL:
         "od_timing": (ci, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd), ctypes.POINTER(ctypes.c_longlong)]),
         "od_last_error": (ctypes.c_char_p, [vp]),
         "od_fr_tables": (ci, [vp]),
+        "od_rhs_noalloc": (ci, [P, vp, vp, sz, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -108,6 +108,10 @@ double in_type(bool dbl, double x) { return dbl ? x : (double)(float)x; }
 
 }  // namespace
 
+namespace od {
+TablesD host_fr_tables() { return build_tables(); }
+}  // namespace od
+
 struct od_ctx {
     od_params p{};
     od::Combo combo = od::kF32;
