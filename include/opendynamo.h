@@ -122,6 +122,14 @@ int od_launches_per_step(const od_ctx* ctx);
  * not depend on it; the autotuner picks it per mesh and precision. */
 int od_set_launch_shape(od_ctx* ctx, int elems_per_block_a, int elems_per_block_b);
 
+/* z-slab pipeline: each stage runs phase A slab by slab on the context's
+ * stream and phase B of a slab on a second stream as soon as its z
+ * neighbours are done, overlapping phase B's memory traffic with phase A's
+ * arithmetic. slabs = 1 disables it, 0 restores the default (1: on B200 the
+ * pipeline measured slower, phase A alone already fills every SM). Results
+ * do not depend on it. */
+int od_set_pipeline_slabs(od_ctx* ctx, int slabs);
+
 /* Per-kernel timing: when enabled, every stage records CUDA events around its
  * phase-A and phase-B kernels; od_timing sums the recorded intervals since the
  * last reset (synchronizes the stream). */
@@ -136,10 +144,11 @@ int od_timing(od_ctx* ctx, double* ms_phase_a, double* ms_phase_b, long long* n_
  * memory, or fixed-footprint loops. The caller passes the state (d_state, 5
  * planes of u_real) and the output (d_rhs, same size, not aliasing d_state) in
  * device memory; the result equals od_rhs on a context with the same params.
- * The kernels' only scratch, the per-face viscous fluxes, lives in one static
- * device array of OD_NOALLOC_SCRATCH_BYTES per GPU (held until exit), which
- * limits the mesh to OD_NOALLOC_SCRATCH_BYTES / (384 * sizeof(compute type))
- * elements (10922 in f32 compute, 5461 in f64); larger meshes return
+ * The kernels' only scratch, the per-face viscous and interface fluxes, lives
+ * in one static device array of OD_NOALLOC_SCRATCH_BYTES per GPU (held until
+ * exit), which limits the mesh to OD_NOALLOC_SCRATCH_BYTES /
+ * (624 * sizeof(compute type)) elements (6721 in f32 compute, 3360 in f64);
+ * larger meshes return
  * OD_ERR_SCRATCH. All calls share the array: calls whose kernels overlap on
  * the GPU race, so order them on one stream. The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) and sets the kernels'

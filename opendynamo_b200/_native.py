@@ -21,7 +21,7 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "size mismatch", -4: "ca
 EXPORTS = (
     "od_default_params", "od_create", "od_destroy", "od_state_bytes", "od_set_state", "od_get_state",
     "od_set_state_device", "od_get_state_device", "od_step", "od_rhs", "od_sync", "od_stream",
-    "od_launches_per_step", "od_set_launch_shape", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
+    "od_launches_per_step", "od_set_launch_shape", "od_set_pipeline_slabs", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
     "od_rhs_noalloc",
 )
 
@@ -71,6 +71,7 @@ def lib() -> ctypes.CDLL:
         "od_stream": (vp, [vp]),
         "od_launches_per_step": (ci, [vp]),
         "od_set_launch_shape": (ci, [vp, ci, ci]),
+        "od_set_pipeline_slabs": (ci, [vp, ci]),
         "od_set_timing": (ci, [vp, ci]),
         "od_timing": (ci, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd), ctypes.POINTER(ctypes.c_longlong)]),
         "od_last_error": (ctypes.c_char_p, [vp]),

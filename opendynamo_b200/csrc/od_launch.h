@@ -37,8 +37,9 @@ struct StageLaunch {
     int flux;            // 0 slau2, 1 ausm+, 2 rusanov
     int epb_a, epb_b;    // elements per block of phase A / phase B
     bool fast_math;      // approximate f32 division / square root (the reference's default build)
-    bool phase_b;        // launch phase B (viscous neighbour term)
-    cudaEvent_t ev[3];   // optional timing events: before A, between A and B, after B
+    int phases;          // 1 = phase A, 2 = phase B, 3 = both (one stream)
+    long long e0, e1;    // element range (a z-slab: elements are z-major)
+    cudaEvent_t ev[3];   // optional timing events: before A, after A, after B
 };
 
 // Precision combination ids: stored type / state arithmetic / flux arithmetic

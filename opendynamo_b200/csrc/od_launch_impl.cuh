@@ -23,6 +23,7 @@ Tab<T> cast_tab(const TablesD& t) {
 template <class S, class P, class C, class M, int FLUX, int EPB>
 cudaError_t launch_a(const StageAParams<S, P, C>& A, long long nelem, cudaStream_t s) {
     const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
+    if (grid == 0) return cudaSuccess;
     const size_t smem = sizeof(SlotA<P, C>) * EPB;
     stage_a_kernel<S, P, C, M, FLUX, EPB><<<grid, LPE * EPB, smem, s>>>(A);
     return cudaGetLastError();
@@ -46,6 +47,7 @@ cudaError_t launch_a_flux(const StageAParams<S, P, C>& A, int flux, long long ne
 template <class S, class P, class C, int EPB>
 cudaError_t launch_b(const StageBParams<S, P, C>& B, long long nelem, cudaStream_t s) {
     const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
+    if (grid == 0) return cudaSuccess;
     stage_b_kernel<S, P, C, EPB><<<grid, LPE * EPB, 0, s>>>(B);
     return cudaGetLastError();
 }
@@ -61,6 +63,7 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.u0 = (const S*)L.u0;
     A.u_out = (S*)(L.rhs ? L.rhs : L.u_out);
     A.fv = (C*)L.fv;
+    A.fi = (C*)L.fv + L.nelem * 6 * 4 * NF;
     A.m.nx = L.nx;
     A.m.ny = L.ny;
     A.m.nz = L.nz;
@@ -76,25 +79,31 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.mu = (C)L.mu;
     A.forcing = (C)L.forcing;
     A.flags = L.flags | (L.rhs ? kDeferRK : 0);
-    if (L.ev[0]) cudaEventRecord(L.ev[0], s);
-    cudaError_t err;
-    if constexpr (has_fast_variant<C>()) {
-        if (L.fast_math)
-            err = launch_a_flux<S, P, C, MathFast>(A, L.flux, L.nelem, L.epb_a, s);
-        else
-            err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, L.nelem, L.epb_a, s);
-    } else {
-        err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, L.nelem, L.epb_a, s);
+    A.e0 = L.e0;
+    A.e1 = L.e1;
+    const long long count = L.e1 - L.e0;
+    cudaError_t err = cudaSuccess;
+    if (L.phases & 1) {
+        if (L.ev[0]) cudaEventRecord(L.ev[0], s);
+        if constexpr (has_fast_variant<C>()) {
+            if (L.fast_math)
+                err = launch_a_flux<S, P, C, MathFast>(A, L.flux, count, L.epb_a, s);
+            else
+                err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, count, L.epb_a, s);
+        } else {
+            err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, count, L.epb_a, s);
+        }
+        if (err != cudaSuccess) return err;
+        if (L.ev[1]) cudaEventRecord(L.ev[1], s);
     }
-    if (err != cudaSuccess) return err;
-    if (L.ev[1]) cudaEventRecord(L.ev[1], s);
-    if (L.phase_b) {
+    if (L.phases & 2) {
         StageBParams<S, P, C> B;
         B.u_out = (S*)L.u_out;
         B.rhs = (const S*)L.rhs;
         B.u_in = (const S*)L.u_in;
         B.u0 = (const S*)L.u0;
         B.fv = (const C*)L.fv;
+        B.fi = A.fi;
         B.m = A.m;
         B.tc = A.tc;
         for (int d = 0; d < 3; ++d) B.jac[d] = A.jac[d];
@@ -102,13 +111,15 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
         B.rb = A.rb;
         B.rc = A.rc;
         B.flags = A.flags;
+        B.e0 = L.e0;
+        B.e1 = L.e1;
         if (L.epb_b == 8)
-            err = launch_b<S, P, C, 8>(B, L.nelem, s);
+            err = launch_b<S, P, C, 8>(B, count, s);
         else
-            err = launch_b<S, P, C, 16>(B, L.nelem, s);
+            err = launch_b<S, P, C, 16>(B, count, s);
         if (err != cudaSuccess) return err;
+        if (L.ev[2]) cudaEventRecord(L.ev[2], s);
     }
-    if (L.ev[2]) cudaEventRecord(L.ev[2], s);
     return cudaSuccess;
 }
 

@@ -8,8 +8,9 @@
 // fixed-footprint loops that must not grow their memory after start-up. For
 // them this entry point needs no context and calls no cudaMalloc, cudaFree or
 // allocating library routine: the caller passes the state and the output,
-// and the only scratch the kernels need — the per-face viscous fluxes phase
-// B reads from the neighbours — lives in the static device array below.
+// and the only scratch the kernels need — the per-face viscous and interface
+// fluxes phase B reads from the neighbours — lives in the static device
+// array below.
 //
 // The array is OD_NOALLOC_SCRATCH_BYTES (16 MiB) in every GPU that loads the
 // library, held until the process exits. All calls share it and it keeps the
@@ -62,8 +63,9 @@ extern "C" int od_rhs_noalloc(const od_params* p, const void* d_state, void* d_r
     const long long nelem = (long long)p->nx * p->ny * p->nz;
     if ((size_t)nelem * 64 * 5 * (s_double ? 8 : 4) != bytes) return OD_ERR_SIZE;
     if (d_state == d_rhs) return OD_ERR_ARG;
-    // viscous face fluxes: 6 faces x 4 components x 16 points per element
-    const size_t scratch = (size_t)nelem * 6 * 4 * 16 * (c_double ? 8 : 4);
+    // viscous face fluxes (6 faces x 4 components) and minus-face interface
+    // fluxes (3 faces x 5 components), 16 points each, per element
+    const size_t scratch = (size_t)nelem * (6 * 4 + 3 * 5) * 16 * (c_double ? 8 : 4);
     if (scratch > (size_t)OD_NOALLOC_SCRATCH_BYTES) return OD_ERR_SCRATCH;
 
     int prev = 0;
@@ -131,7 +133,9 @@ extern "C" int od_rhs_noalloc(const od_params* p, const void* d_state, void* d_r
     L.flux = p->flux;
     L.epb_a = 4;
     L.epb_b = 16;
-    L.phase_b = p->mu != 0.0;
+    L.phases = 3;
+    L.e0 = 0;
+    L.e1 = nelem;
     L.fast_math = p->fast_math != 0;
     cudaError_t e = launch(L, (cudaStream_t)stream);
     cudaSetDevice(prev);

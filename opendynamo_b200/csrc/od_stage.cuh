@@ -197,6 +197,7 @@ struct StageAParams {
     const S* u0;
     S* u_out;       // new state, or the RHS when phase B performs the RK combination
     C* fv;          // [elem][face 6][var 4][face pt 16]: own viscous face flux, components 1..4
+    C* fi;          // [elem][dir 3][var 5][face pt 16]: interface flux of the element's minus faces
     Mesh m;
     Tab<P> tp;
     Tab<C> tc;
@@ -204,32 +205,51 @@ struct StageAParams {
     P ra, rb, rc;
     C mu, forcing;
     int flags;
+    long long e0, e1;   // element range of this launch
 };
 
-// Interface-flux part of the face correction at one face point, side `side`
-// of direction D: j = F_I - Fe_own, or the slip-wall flux minus Fe_own.
+// Inviscid part of the face corrections at the two faces of a line. Each
+// face's interface flux F_I is solved once, by the element on its plus side
+// (the face is that element's minus face): there j = F_I - Fe_own and F_I is
+// stored for the neighbour; on the element's plus face j = -Fe_own here and
+// phase B adds the neighbour's F_I. Slip walls (rhs.cu:311-339) are complete
+// here: j = [0, 0, p_wall, 0, 0] - Fe_own with p_wall from the own flux.
+template <class M, int D, class P, class C>
+__device__ __forceinline__ void wall_face(const FaceState<C>& so, const C* fe, C* j) {
+    const C pw = fe[2] - so.q[2] * so.q[2] * so.ir;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) j[v] = -fe[v];
+    j[2] = pw - fe[2];
+}
+
 template <class M, int FLUX, int D, class P, class C>
-__device__ __forceinline__ void inviscid_face(const P* own, const P* nbr, int side, bool wall, C* j) {
+__device__ __forceinline__ void minus_face(const P* own, const P* nbr, bool wall, C* j, C* fi) {
     C praw;
     FaceState<C> so = make_face_state<M, C, P>(own, praw);
     C fe[NV];
     euler_flux<D>(so, fe);
     if (wall) {
-        // F_wall = [0, 0, p_wall, 0, 0], p_wall from the own flux (rhs.cu:321-326)
-        const C pw = fe[2] - so.q[2] * so.q[2] * so.ir;
-#pragma unroll
-        for (int v = 0; v < NV; ++v) j[v] = -fe[v];
-        j[2] = pw - fe[2];
+        wall_face<M, D, P, C>(so, fe, j);
         return;
     }
     FaceState<C> sn = make_face_state<M, C, P>(nbr, praw);
-    C fi[NV];
-    if (side)
-        interface_flux<M, FLUX, D>(so, sn, fi);
-    else
-        interface_flux<M, FLUX, D>(sn, so, fi);
+    interface_flux<M, FLUX, D>(sn, so, fi);
 #pragma unroll
     for (int v = 0; v < NV; ++v) j[v] = fi[v] - fe[v];
+}
+
+template <class M, int D, class P, class C>
+__device__ __forceinline__ void plus_face(const P* own, bool wall, C* j) {
+    C praw;
+    FaceState<C> so = make_face_state<M, C, P>(own, praw);
+    C fe[NV];
+    euler_flux<D>(so, fe);
+    if (wall) {
+        wall_face<M, D, P, C>(so, fe, j);
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) j[v] = -fe[v];
 }
 
 // load / store the 4 samples of line l in direction D of a swizzled row
@@ -256,12 +276,13 @@ __device__ __forceinline__ void row_line_store(T* row, int l, int swz, const T* 
 // P2-P4: one direction of the gradient / face-value pass for line l.
 template <class M, int FLUX, int D, class S, class P, class C>
 __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, int l, int swz,
-                                          const long long nb0, const long long nb1) {
+                                          const long long nb0, const long long nb1, long long e, bool live,
+                                          P* oL, P* oR) {
     const Mesh& m = A.m;
     P q[NV][4];
 #pragma unroll
     for (int v = 0; v < NV; ++v) row_line_load<D>(sm.u[v], l, swz, q[v]);
-    P oL[NV], oR[NV], nL[NV], nR[NV];
+    P nL[NV], nR[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         oL[v] = trace4(q[v], A.tp.eL);
@@ -317,10 +338,15 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
         }
         row_line_store<D>(sm.g[3 * v + D], l, swz, gv);
     }
-    // interface fluxes at the two faces of this line
-    C j0[NV], j1[NV];
-    inviscid_face<M, FLUX, D, P, C>(oL, nL, 0, nb0 < 0, j0);
-    inviscid_face<M, FLUX, D, P, C>(oR, nR, 1, nb1 < 0, j1);
+    // inviscid parts at the two faces of this line
+    C j0[NV], j1[NV], fi[NV];
+    minus_face<M, FLUX, D, P, C>(oL, nL, nb0 < 0, j0, fi);
+    plus_face<M, D, P, C>(oR, nb1 < 0, j1);
+    if (live && nb0 >= 0) {
+        C* out = A.fi + ((e * 3 + D) * NV) * NF + l;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v * NF] = fi[v];
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         sm.j[2 * D][v][l] = j0[v];
@@ -361,7 +387,8 @@ __device__ __forceinline__ C ref_y_slice(const C* w, const C* c) {
 // flux at both faces of the line.
 template <class M, int D, class S, class P, class C>
 __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
-                                               int swz, bool wall0, bool wall1, bool live) {
+                                               int swz, bool wall0, bool wall1, bool live, const P* tL,
+                                               const P* tR) {
     if (wall0 && wall1) return;
     C gL[15], gR[15];
     const bool ref_y = D == 1 && sizeof(C) == 8 && (A.flags & kRefYSlice);
@@ -382,13 +409,19 @@ __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, S
             gR[c] = trace4(w, A.tc.eR);
         }
     }
+    // face values: kept in registers from the line pass (f32), else recomputed
     P qL[NV], qR[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        P w[4];
-        row_line_load<D>(sm.u[v], l, swz, w);
-        qL[v] = trace4(w, A.tp.eL);
-        qR[v] = trace4(w, A.tp.eR);
+        if constexpr (sizeof(P) == 4) {
+            qL[v] = tL[v];
+            qR[v] = tR[v];
+        } else {
+            P w[4];
+            row_line_load<D>(sm.u[v], l, swz, w);
+            qL[v] = trace4(w, A.tp.eL);
+            qR[v] = trace4(w, A.tp.eR);
+        }
     }
     if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live);
     if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live);
@@ -420,8 +453,8 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
     const int es = threadIdx.x / LPE;
     const int swz = (es & 1) << 3;
     SlotA<P, C>& sm = reinterpret_cast<SlotA<P, C>*>(smem_raw)[es];
-    const long long e = (long long)blockIdx.x * EPB + es;
-    const bool live = e < A.m.nelem;
+    const long long e = A.e0 + (long long)blockIdx.x * EPB + es;
+    const bool live = e < A.e1;
     const long long ec = live ? e : 0;
     const Mesh& m = A.m;
     const int ex = (int)(ec % m.nx);
@@ -446,15 +479,16 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
     __syncthreads();
 
     // ---- P2-P4: face values, gradient, interface fluxes per direction
-    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp);
-    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp);
-    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp);
+    P tr[3][2][NV];   // own face values of this thread's lines (kept only for f32 state arithmetic)
+    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp, ec, live, tr[0][0], tr[0][1]);
+    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp, ec, live, tr[1][0], tr[1][1]);
+    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp, ec, live, tr[2][0], tr[2][1]);
     __syncthreads();
 
     // ---- P5: viscous face fluxes of all six faces
-    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live);
-    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live);
-    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live);
+    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live, tr[0][0], tr[0][1]);
+    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live, tr[1][0], tr[1][1]);
+    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live, tr[2][0], tr[2][1]);
     __syncthreads();
 
     // ---- P6: pointwise fluxes of the x-line's points (own points only; the
@@ -549,22 +583,28 @@ struct StageBParams {
     const S* u_in;
     const S* u0;
     const C* fv;
+    const C* fi;
     Mesh m;
     Tab<C> tc;
     C jac[3];
     P ra, rb, rc;
     int flags;
+    long long e0, e1;   // element range of this launch
 };
 
-// Phase B: rc * lift(-1/2 Fv_nbr) over the element's non-wall faces, added to
-// the new state, or (deferred RK) u_out = ra*u0 + rb*u_in + rc*(RHS + lift).
-// 16 threads per element, each the x-line l = j + 4k (128-bit accesses).
+// Phase B: the neighbour-dependent part of the face corrections,
+//   plus faces:  j += F_I (solved by the plus neighbour) - 1/2 Fv_nbr
+//   minus faces: j += -1/2 Fv_nbr
+// lifted with -(j g') jac (rk.cu:12-25) over the element's non-wall faces and
+// added to the new state (times rc), or (deferred RK) folded into
+// u_out = ra*u0 + rb*u_in + rc*(RHS + lift). 16 threads per element, each the
+// x-line l = j + 4k (128-bit accesses).
 template <class S, class P, class C, int EPB>
 __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
     const int l = threadIdx.x & (LPE - 1);
-    const long long e = (long long)blockIdx.x * EPB + threadIdx.x / LPE;
+    const long long e = B.e0 + (long long)blockIdx.x * EPB + threadIdx.x / LPE;
     const Mesh& m = B.m;
-    if (e >= m.nelem) return;
+    if (e >= B.e1) return;
     const int ex = (int)(e % m.nx);
     const int ey = (int)((e / m.nx) % m.ny);
     const int ez = (int)(e / ((long long)m.nx * m.ny));
@@ -574,55 +614,62 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
     const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
     const C hx = (C)0.5 * B.jac[0], hy = (C)0.5 * B.jac[1], hz = (C)0.5 * B.jac[2];
     const bool defer = (B.flags & kDeferRK) != 0;
-    if (defer) {
-        // density has no viscous term: only the RK combination
-        const long long off = e * NE + 4 * l;
-        C r[4];
-        P un[4], u0v[4], out[4];
-        ldg4<S, C>(B.rhs + off, r);
-        ldg4<S, P>(B.u_in + off, un);
-        if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, u0v);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            P o = B.rb * un[i] + B.rc * (P)r[i];
-            if (B.flags & kHasU0) o = B.ra * u0v[i] + B.rb * un[i] + B.rc * (P)r[i];
-            out[i] = o;
-        }
-        stg4<S, P>(B.u_out + off, out);
-    }
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < NV; ++v) {
         C acc[4] = {(C)0, (C)0, (C)0, (C)0};
-        // the neighbour's record of the shared face is its opposite side
+        // interface fluxes of the plus faces: the plus neighbour's minus-face record
         {
-            const C a0 = __ldg(B.fv + ((nxm * 6 + 1) * 4 + v) * NF + l);
-            const C a1 = __ldg(B.fv + ((nxp * 6 + 0) * 4 + v) * NF + l);
+            const C f0 = __ldg(B.fi + ((nxp * 3 + 0) * NV + v) * NF + l);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, fma(hx * B.tc.gR[i], a1, acc[i]));
-        }
-        if (nym >= 0) {
-            C w[4];
-            ld4s(B.fv + ((nym * 6 + 3) * 4 + v) * NF + 4 * lk, w);
-            const C c = hy * B.tc.gL[lj];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+            for (int i = 0; i < 4; ++i) acc[i] = fma(-B.jac[0] * B.tc.gR[i], f0, acc[i]);
         }
         if (nyp >= 0) {
             C w[4];
-            ld4s(B.fv + ((nyp * 6 + 2) * 4 + v) * NF + 4 * lk, w);
-            const C c = hy * B.tc.gR[lj];
+            ld4s(B.fi + ((nyp * 3 + 1) * NV + v) * NF + 4 * lk, w);
+            const C c = -B.jac[1] * B.tc.gR[lj];
 #pragma unroll
             for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
         }
         {
-            C w0[4], w1[4];
-            ld4s(B.fv + ((nzm * 6 + 5) * 4 + v) * NF + 4 * lj, w0);
-            ld4s(B.fv + ((nzp * 6 + 4) * 4 + v) * NF + 4 * lj, w1);
-            const C c0 = hz * B.tc.gL[lk], c1 = hz * B.tc.gR[lk];
+            C w[4];
+            ld4s(B.fi + ((nzp * 3 + 2) * NV + v) * NF + 4 * lj, w);
+            const C c = -B.jac[2] * B.tc.gR[lk];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(c0, w0[i], fma(c1, w1[i], acc[i]));
+            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
         }
-        const long long off = (v + 1) * m.npts + e * NE + 4 * l;
+        if (v > 0) {
+            // viscous: the neighbour's record of the shared face is its opposite side
+            const int q = v - 1;
+            {
+                const C a0 = __ldg(B.fv + ((nxm * 6 + 1) * 4 + q) * NF + l);
+                const C a1 = __ldg(B.fv + ((nxp * 6 + 0) * 4 + q) * NF + l);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, fma(hx * B.tc.gR[i], a1, acc[i]));
+            }
+            if (nym >= 0) {
+                C w[4];
+                ld4s(B.fv + ((nym * 6 + 3) * 4 + q) * NF + 4 * lk, w);
+                const C c = hy * B.tc.gL[lj];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+            }
+            if (nyp >= 0) {
+                C w[4];
+                ld4s(B.fv + ((nyp * 6 + 2) * 4 + q) * NF + 4 * lk, w);
+                const C c = hy * B.tc.gR[lj];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+            }
+            {
+                C w0[4], w1[4];
+                ld4s(B.fv + ((nzm * 6 + 5) * 4 + q) * NF + 4 * lj, w0);
+                ld4s(B.fv + ((nzp * 6 + 4) * 4 + q) * NF + 4 * lj, w1);
+                const C c0 = hz * B.tc.gL[lk], c1 = hz * B.tc.gR[lk];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc[i] = fma(c0, w0[i], fma(c1, w1[i], acc[i]));
+            }
+        }
+        const long long off = v * m.npts + e * NE + 4 * l;
         P out[4];
         if (defer) {
             C r[4];

@@ -134,6 +134,10 @@ class Solver:
     def set_launch_shape(self, epb_a: int, epb_b: int) -> None:
         self._chk(self._lib.od_set_launch_shape(self._ctx, int(epb_a), int(epb_b)), "od_set_launch_shape")
 
+    def set_pipeline_slabs(self, slabs: int) -> None:
+        """z-slabs per stage of the phase-A / phase-B pipeline (1 = off, 0 = auto)."""
+        self._chk(self._lib.od_set_pipeline_slabs(self._ctx, int(slabs)), "od_set_pipeline_slabs")
+
     def set_timing(self, enabled: bool) -> None:
         self._chk(self._lib.od_set_timing(self._ctx, int(enabled)), "od_set_timing")
 

@@ -128,6 +128,28 @@ def test_restart_bit_exact(prec):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_slab_pipeline_and_launch_shape_do_not_change_results(prec):
+    """The z-slab pipeline (phase B of a slab on a second stream) and the
+    block shapes change scheduling only: byte-identical states."""
+    dtype = np.float64 if prec == "f64" else np.float32
+    mesh = (4, 3, 8)
+    u = channel_trip(*mesh, amp=0.02, dtype=dtype)
+    _, dp = _pair(mesh, "slau2", True, prec)
+    dt = float(np.float32(1e-3))
+    outs = []
+    for slabs, ea, eb in ((1, 4, 16), (2, 2, 8), (4, 4, 8), (8, 2, 16)):
+        with Solver(dp) as s:
+            s.set_pipeline_slabs(slabs)
+            s.set_launch_shape(ea, eb)
+            s.set_state(u)
+            s.step(6, dt)
+            outs.append(s.get_state())
+    for o in outs[1:]:
+        assert o.tobytes() == outs[0].tobytes()
+
+
+@pytest.mark.gpu
 def test_mixed_precision_beats_f32():
     """Precision form (f64 state/RK/pressure, f32 fluxes) vs the f64 oracle:
     its error must be below the all-f32 pipeline's."""
