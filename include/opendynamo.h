@@ -162,6 +162,87 @@ int od_rhs_noalloc(const od_params* params, const void* d_state, void* d_rhs, si
 /* Message of the last failure on this context ("" if none). */
 const char* od_last_error(const od_ctx* ctx);
 
+/* ------------------------------------------------------------------------
+ * Solver-native state files (HDF5; src/io.rs). Host-only, no device work.
+ * A file holds /data/{rho,rhou,rhov,rhow,E} as 1-D datasets of nx*ny*nz*64
+ * values of the state type, plus root attributes nx ny nz fr_order step
+ * (u64), t lx ly lz (f64) and u_real ("f32"/"f64", fixed 3-byte ASCII).
+ * The writer emits the HDF5 "earliest" format libhdf5 writes by default;
+ * the reader accepts that format as libhdf5 writes it (continuation blocks,
+ * multi-level chunk indexes). Errors are kept per thread (od_state_error).
+ * ------------------------------------------------------------------------ */
+
+/* Write a state file (atomically: <path>.tmp, then rename).
+ * planes: 5 planes of the state type (u_f64 ? double : float), var-major as
+ * the device holds them. compression: "none" (contiguous), "gzip1".."gzip9"
+ * (262144-element chunks, shuffle + deflate), "blosc-lz4" (clevel 9) or
+ * "blosc-zstd" (clevel 5) (HDF5 filter 32001, byte shuffle; needs
+ * liblz4.so.1 / libzstd.so.1 at run time). lx, ly, lz: the f32 extents
+ * widened, as the reference stores them.
+ * Replaces: save_state_h5 (src/io.rs:59-136) and parse_compression
+ * (src/io.rs:32-52); same file layout, attributes and error text. */
+int od_state_save(const char* path, const void* planes, int u_f64, int nx, int ny, int nz,
+                  unsigned long long step, double t, double lx, double ly, double lz,
+                  const char* compression);
+
+/* Read a state file's attributes (any pointer may be null). u_real4 receives
+ * the precision tag, NUL-terminated. */
+int od_state_info(const char* path, int* nx, int* ny, int* nz, int* fr_order,
+                  unsigned long long* step, double* t, double* lx, double* ly, double* lz,
+                  char* u_real4);
+
+/* Validating load into planes_out (bytes = 5 * nx*ny*nz*64 * sizeof(state
+ * type)): the file's mesh, fr_order (3) and u_real must match, else
+ * OD_ERR_SIZE with the reference's message. Returns the file's step label
+ * and time. Planes are read in their stored type: an f64 file loads exactly
+ * (the reference reads every plane through f32, src/io.rs:221, so its f64
+ * resume rounds; here it is exact).
+ * Replaces: load_state_h5 (src/io.rs:163-234). */
+int od_state_load(const char* path, void* planes_out, size_t bytes, int expect_u_f64,
+                  int nx, int ny, int nz, unsigned long long* step, double* t);
+
+/* Message of this thread's last state-file failure. */
+const char* od_state_error(void);
+
+/* ------------------------------------------------------------------------
+ * Run driver: the reference's run loop (src/solver.rs:139-374, 745-818) on
+ * top of the entry points above. Loads [physics].initial_state, writes the
+ * startup state as label S (the file's own label) at t = base_t, runs
+ * n_steps SSP-RK3 steps, and after loop step k (0-based) with
+ * k % save_freq == 0 or k == n_steps-1 writes <output_dir>/<prefix>_<u_real>
+ * _<label:06>.h5 with label = S + k + 1 and t = base_t + (k + 1) * dt; the
+ * same state also goes to checkpoint_<u_real>_<label:06>.h5 when
+ * k == n_steps-1 or (checkpoint_freq > 0 and k % checkpoint_freq == 0).
+ * Dumps are asynchronous: a device-side snapshot, a copy to one of three
+ * pinned host buffers on a second stream and a host thread per file, so the
+ * step loop waits only when all three buffers are in flight. As in the
+ * reference, a failed file write is reported on stderr and the run
+ * continues (counted in io_errors).
+ * ------------------------------------------------------------------------ */
+typedef struct od_run_opts {
+    const char* initial_state;     /* [physics] initial_state (required) */
+    long long n_steps;             /* [solver] n_steps */
+    double dt;                     /* [solver] dt: the f32 value widened */
+    long long save_freq;           /* [io] save_freq (> 0) */
+    long long checkpoint_freq;     /* [io] checkpoint_freq (0 = final step only) */
+    const char* compression;       /* [io] compression */
+    const char* output_dir;        /* [io] output_dir (created if missing) */
+    const char* prefix;            /* [io] prefix */
+    int quiet;                     /* 1 = no progress lines on stdout */
+} od_run_opts;
+
+typedef struct od_run_result {
+    unsigned long long start_label, final_label;
+    double start_t, final_t;
+    double seconds;                /* wall time of the step loop incl. waiting for the dumps */
+    double ms_per_step;
+    long long files_written, io_errors;
+    float rho_min, rho_max, u_min, u_max; /* final physical-state report (f32, solver.rs:820-840) */
+} od_run_result;
+
+/* Run. err (may be null) receives the failure message. */
+int od_run(const od_params* p, const od_run_opts* o, od_run_result* r, char* err, size_t err_len);
+
 /* FR P=3 operator tables in double, as src/fr_math.rs:107-142 builds them:
  * points[4], D[16] (D[i*4+j] = l'_j(x_i)), extrap_left[4], extrap_right[4],
  * g_left'[4], g_right'[4]. */

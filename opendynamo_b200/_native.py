@@ -22,7 +22,7 @@ EXPORTS = (
     "od_default_params", "od_create", "od_destroy", "od_state_bytes", "od_set_state", "od_get_state",
     "od_set_state_device", "od_get_state_device", "od_step", "od_rhs", "od_sync", "od_stream",
     "od_launches_per_step", "od_set_launch_shape", "od_set_pipeline_slabs", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
-    "od_rhs_noalloc",
+    "od_rhs_noalloc", "od_state_save", "od_state_info", "od_state_load", "od_state_error", "od_run",
 )
 
 
@@ -36,6 +36,26 @@ class OdParams(ctypes.Structure):
         ("mixed", ctypes.c_int), ("fast_math", ctypes.c_int),
         ("mu", ctypes.c_double), ("forcing", ctypes.c_double),
         ("device", ctypes.c_int), ("ref_compat", ctypes.c_int),
+    ]
+
+
+class OdRunOpts(ctypes.Structure):
+    _fields_ = [
+        ("initial_state", ctypes.c_char_p), ("n_steps", ctypes.c_longlong), ("dt", ctypes.c_double),
+        ("save_freq", ctypes.c_longlong), ("checkpoint_freq", ctypes.c_longlong),
+        ("compression", ctypes.c_char_p), ("output_dir", ctypes.c_char_p), ("prefix", ctypes.c_char_p),
+        ("quiet", ctypes.c_int),
+    ]
+
+
+class OdRunResult(ctypes.Structure):
+    _fields_ = [
+        ("start_label", ctypes.c_ulonglong), ("final_label", ctypes.c_ulonglong),
+        ("start_t", ctypes.c_double), ("final_t", ctypes.c_double),
+        ("seconds", ctypes.c_double), ("ms_per_step", ctypes.c_double),
+        ("files_written", ctypes.c_longlong), ("io_errors", ctypes.c_longlong),
+        ("rho_min", ctypes.c_float), ("rho_max", ctypes.c_float),
+        ("u_min", ctypes.c_float), ("u_max", ctypes.c_float),
     ]
 
 
@@ -77,6 +97,15 @@ def lib() -> ctypes.CDLL:
         "od_last_error": (ctypes.c_char_p, [vp]),
         "od_fr_tables": (ci, [vp]),
         "od_rhs_noalloc": (ci, [P, vp, vp, sz, vp]),
+        "od_state_save": (ci, [ctypes.c_char_p, vp, ci, ci, ci, ci, ctypes.c_ulonglong, cd, cd, cd, cd,
+                               ctypes.c_char_p]),
+        "od_state_info": (ci, [ctypes.c_char_p, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci),
+                               ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(cd),
+                               ctypes.POINTER(cd), ctypes.POINTER(cd), ctypes.POINTER(cd), ctypes.c_char_p]),
+        "od_state_load": (ci, [ctypes.c_char_p, vp, sz, ci, ci, ci, ci, ctypes.POINTER(ctypes.c_ulonglong),
+                               ctypes.POINTER(cd)]),
+        "od_state_error": (ctypes.c_char_p, []),
+        "od_run": (ci, [P, ctypes.POINTER(OdRunOpts), ctypes.POINTER(OdRunResult), ctypes.c_char_p, sz]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

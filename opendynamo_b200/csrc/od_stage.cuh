@@ -13,8 +13,10 @@
 //   P1  the element state (x-lines, 128-bit loads) -> smem
 //   P2-4 per direction: own and neighbour face values (BR1 common solution,
 //        slip-wall mirror rhs.cu:111-114), corrected gradient along the line
-//        (rhs.cu:373-461), interface flux F_I and own Euler flux at the two
-//        faces of the line -> j = F_I - Fe_own (slip wall: [0,0,p_w,0,0] - Fe)
+//        (rhs.cu:373-461); at the minus face of the line the interface flux
+//        F_I is solved once for both sides (j = F_I - Fe_own here, F_I kept
+//        in the face buffer for the minus neighbour); at the plus face
+//        j = -Fe_own (slip wall: j = [0,0,p_w,0,0] - Fe, complete)
 //   P5  x / y / z faces: gradient at the face (11 components), own viscous
 //        flux Fv; j += 1/2 Fv_own; Fv_own -> face buffer for the neighbour
 //   P6  x-threads: pointwise Euler - viscous fluxes of their 4 points
@@ -24,15 +26,17 @@
 //        -(j_L g_L' + j_R g_R') jac (rk.cu:12-25), RK combination
 //        a*u0 + b*u + c*(RHS + lift) (rk.cu:27-83), 128-bit stores.
 //   The face correction of the reference, j = F_I - 1/2(Fv_L + Fv_R) -
-//   (Fe_own - Fv_own), is complete here except for -1/2 Fv_nbr.
-// Phase B — adds c * lift(-1/2 Fv_nbr) over the element's non-wall faces.
-// With an f32 state phase A stores the unrounded RHS instead of the new state
-// and phase B performs the RK combination, so the state is rounded once per
-// stage: phase B's increments are often below half an f32 ulp of E and rho*u,
-// and rounding the state before adding them would drop them systematically.
-// Only the neighbour's viscous face flux depends on the neighbour's
-// gradient (hence on its own neighbours); everything else is element-local
-// given the six neighbours' face values. Phase B is skipped when mu == 0.
+//   (Fe_own - Fv_own), is then complete except for the terms that belong to
+//   the neighbour: F_I at the plus faces and -1/2 Fv_nbr at every non-wall
+//   face.
+// Phase B — reads those from the face buffer records of the +x/+y/+z and
+// -x/-y/-z neighbours and adds their lifted contribution. With an f32 state
+// phase A stores the unrounded RHS instead of the new state and phase B
+// performs the RK combination, so the state is rounded once per stage:
+// phase B's increments are often below half an f32 ulp of E and rho*u, and
+// rounding the state before adding them would drop them systematically.
+// Phase B always runs (the plus-face F_I comes from the neighbour even when
+// mu == 0).
 //
 // Types: S = stored state, P = state arithmetic (face values, pressure
 // recovery, RK accumulation), C = flux arithmetic. Reference-compatible
