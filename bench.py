@@ -286,6 +286,96 @@ def run_reference(args, world, rank, local):
     return ref_harness.bench_line(args, WORKLOAD, RK_PER_STEP, METRIC, BYTES_PER_DOF_STAGE)
 
 
+def run_precision_form(args, world, rank, local):
+    """Precision form (FP32 fluxes, FP64 state / RK / pressure) on the 96^3
+    channel: errors, KE / enstrophy drift and throughput of the all-FP64,
+    mixed and all-FP32 pipelines from one initial state."""
+    if rank != 0:
+        return None
+    import torch
+    from opendynamo_b200.forms.precision import precision_study
+    torch.cuda.set_device(local)
+    n = args.mesh or 96
+    steps = args.form_steps or 2000
+    res = precision_study(n=n, steps=steps, dt=1e-4 * 96 / n, chunk=max(1, steps // 20), device=local)
+    mixed = res["pipelines"]["mixed"]
+    return {"metric": f"Gdof*stage/s, precision form (channel {n}^3, FP32 flux, FP64 state/RK/pressure)",
+            "value": mixed["gdof_stage_s"], "unit": "Gdof*stage/s", "n_gpus": 1, "steps": steps,
+            "higher_is_better": True, "dtype": "f64 state / f32 flux", "data": "synthetic (channel IC, seed 42)",
+            "config": {"workload": f"channel {n}^3 elements, SLAU2, y slip walls", "form": "precision"},
+            "study": res}
+
+
+def run_ensemble_form(args, world, rank, local):
+    """Batching form: the 64-box ensemble (seed 7) in one persistent launch
+    per RK stage (autotuned, CUDA graph) against looping single instances."""
+    if rank != 0:
+        return None
+    import torch
+    from opendynamo_b200.forms.ensemble import benchmark_boxes, compare_with_loop
+    torch.cuda.set_device(local)
+    boxes = benchmark_boxes()
+    steps = args.form_steps or 20
+    res = compare_with_loop(boxes, steps=steps, warmup=args.warmup, device=local)
+    return {"metric": "aggregate Gdof*stage/s, 64-box ensemble (8^3-32^3, seed 7), f32",
+            "value": round(res["ensemble_gdof_stage_s"], 3), "unit": "Gdof*stage/s", "n_gpus": 1, "steps": steps,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (TGV / tripped-channel boxes, seed 7)",
+            "config": {"workload": "64 boxes, log-uniform 8^3..32^3, Mach 0.05-0.3, Re 400-1600, Rusanov/SLAU2",
+                       "form": "ensemble"},
+            "loop_value": round(res["loop_gdof_stage_s"], 3), "study": res}
+
+
+def run_closure_form(args, world, rank, local):
+    """Learned-closure form: data from fine runs (4x the coarse mesh per
+    axis), training of the per-element network on the tensor cores, and the
+    held-out comparison of plain coarse / closure coarse / plain 2x runs
+    against the filtered fine run."""
+    if rank != 0:
+        return None
+    import dataclasses  # noqa: F401
+    import torch
+    from opendynamo_b200.forms import closure as CL
+    torch.cuda.set_device(local)
+    cfg = dict(CL.DEFAULT)
+    nc = args.mesh or cfg["coarse"]
+    cfg.update(coarse=nc, mid=2 * nc, fine=4 * nc, dt_fine=1e-4 * 96 / (4 * nc))
+    if args.form_steps:
+        cfg["horizon_steps"] = args.form_steps
+    if args.train_seeds:
+        cfg["train_seeds"] = tuple(range(args.train_seeds))
+    if args.eval_seeds:
+        cfg["eval_seeds"] = tuple(range(100, 100 + args.eval_seeds))
+    if args.snaps:
+        cfg["snaps_per_seed"] = args.snaps
+    if args.epochs:
+        cfg["epochs"] = args.epochs
+    log = lambda m: print(m, file=sys.stderr, flush=True)
+    data = CL.generate_data(cfg, device=local, log=log)
+    net, tr = CL.train(data, cfg, device=local, log=log)
+    norm = {"mean": data["mean"].tolist(), "scale": data["scale"].tolist(), "out_scale": data["out_scale"].tolist()}
+    del data
+    torch.cuda.empty_cache()
+    ev = CL.evaluate(net, cfg, device=local, log=log)
+    if args.save_weights:
+        p = net.get_params()
+        np.savez_compressed(args.save_weights, **p, mean=np.array(norm["mean"], np.float32),
+                            scale=np.array(norm["scale"], np.float32),
+                            out_scale=np.array(norm["out_scale"], np.float32))
+    net.close()
+    w = ev["wall_ms"]
+    speed = w["plain_mid"] / max(w["closure_coarse"], 1e-9)
+    return {"metric": f"closure {nc}^3 vs plain {2 * nc}^3 wall time at equal error (filtered {4 * nc}^3 reference)",
+            "value": round(speed, 3), "unit": "x lower wall time", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32 solver / bf16 network", "data": "synthetic (channel trip ICs; seeds as configured)",
+            "config": {"workload": f"channel coarse {nc}^3, fine {4 * nc}^3, mid {2 * nc}^3, Re_bulk "
+                                   f"{cfg['re_bulk']}, Mach {cfg['mach']}, SLAU2", "form": "closure",
+                       "train_seeds": list(cfg["train_seeds"]), "eval_seeds": list(cfg["eval_seeds"]),
+                       "horizon_steps_fine": cfg["horizon_steps"], "snaps_per_seed": cfg["snaps_per_seed"],
+                       "epochs": cfg["epochs"]},
+            "training": {"history": tr["history"], "train_s": round(tr["train_s"], 2), "steps": tr["steps"]},
+            "evaluation": ev, "normalisation": norm}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -293,12 +383,27 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="plain", choices=["plain", "precision", "ensemble", "closure"],
+                    help="plain: the headline 48^3 bench; precision: the precision-form study")
+    ap.add_argument("--mesh", type=int, default=0, help="elements per axis of a --form run (0 = its default)")
+    ap.add_argument("--form-steps", type=int, default=0, help="RK3 steps of a --form run (0 = its default)")
+    ap.add_argument("--train-seeds", type=int, default=0, help="closure: number of training seeds (0 = 16)")
+    ap.add_argument("--eval-seeds", type=int, default=0, help="closure: number of held-out seeds (0 = 4)")
+    ap.add_argument("--snaps", type=int, default=0, help="closure: snapshots per training seed (0 = 125)")
+    ap.add_argument("--epochs", type=int, default=0, help="closure: training epochs (0 = 8)")
+    ap.add_argument("--save-weights", default="", help="closure: write the trained network (.npz)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = _dist()
     if args.impl == "reference":
         out = run_reference(args, world, rank, local)
+    elif args.form == "precision":
+        out = run_precision_form(args, world, rank, local)
+    elif args.form == "ensemble":
+        out = run_ensemble_form(args, world, rank, local)
+    elif args.form == "closure":
+        out = run_closure_form(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if out is not None and rank == 0:

@@ -60,7 +60,16 @@ typedef struct od_params {
     double forcing;                /* source added to the rho*u RHS; reference 1e-3 (rhs.cu:508) */
     int device;                    /* CUDA device ordinal */
     int ref_compat;                /* OD_COMPAT_* bits: reproduce reference arithmetic quirks (default 0) */
+    int viscosity_model;           /* OD_VISC_CONSTANT (reference) or OD_VISC_SUTHERLAND (extension) */
+    double t_ref, s_suth;          /* Sutherland reference temperature and constant, K ([physics] t_ref
+                                      s_suth; defaults 273.15, 110.4) */
 } od_params;
+
+/* Viscosity models. The reference parses [physics] viscosity_model but its
+ * kernels always use the constant MU_REF (constants.cuh:42); Sutherland's law
+ * mu = mu * T^1.5 (1 + S) / (T + S), T = gamma p / rho, S = s_suth / t_ref,
+ * is an extension selected explicitly. */
+enum { OD_VISC_CONSTANT = 0, OD_VISC_SUTHERLAND = 1 };
 
 /* ref_compat bits. OD_COMPAT_Y_SLICE_F32: the reference builds its y-face
  * gradient slices with __fmul_rn, a float intrinsic, also in its f64
@@ -70,7 +79,7 @@ typedef struct od_params {
  * is f64 throughout (more accurate). */
 enum { OD_COMPAT_Y_SLICE_F32 = 1 };
 
-/* Reference defaults: SLAU2, slip walls, all f32, mu 1.6e-4, forcing 1e-3. */
+/* Reference defaults: SLAU2, slip walls, all f32, mu 1.6e-4 constant, forcing 1e-3. */
 void od_default_params(od_params* p);
 
 /* Allocate device buffers and prepare the kernels.
@@ -162,6 +171,19 @@ int od_rhs_noalloc(const od_params* params, const void* d_state, void* d_rhs, si
 /* Message of the last failure on this context ("" if none). */
 const char* od_last_error(const od_ctx* ctx);
 
+/* Diagnostics of the current state (synchronous). Gauss-Legendre quadrature
+ * of the solution points; the vorticity uses element-local FR derivatives.
+ *   vol6 = { int rho, int rho*u, int E, int 1/2 rho |u|^2,
+ *            int 1/2 rho |curl u|^2, volume }
+ *   prof (may be null; prof_len >= ny*4*8): x-z plane averages at the y of
+ *   every solution-point row (row = 4*ey + j, bottom to top), 8 per row:
+ *   <rho> <u> <v> <w> <u u> <v v> <w w> <u v>, u = rho*u / rho etc. The
+ *   mean profile is <u>; Reynolds stresses are <u u> - <u><u> etc.
+ * No reference counterpart (the reference reports only min/max of rho and
+ * u at the end of a run, solver.rs:820-840); used for the precision-form
+ * drift figures and the closure's evaluation. */
+int od_diagnostics(od_ctx* ctx, double* vol6, double* prof, size_t prof_len);
+
 /* ------------------------------------------------------------------------
  * Solver-native state files (HDF5; src/io.rs). Host-only, no device work.
  * A file holds /data/{rho,rhou,rhov,rhow,E} as 1-D datasets of nx*ny*nz*64
@@ -242,6 +264,103 @@ typedef struct od_run_result {
 
 /* Run. err (may be null) receives the failure message. */
 int od_run(const od_params* p, const od_run_opts* o, od_run_result* r, char* err, size_t err_len);
+
+/* ------------------------------------------------------------------------
+ * Ensembles (the batching form): independent boxes of uneven size, each with
+ * its own extents, flux scheme, viscosity, forcing and time step, advanced
+ * together in the f32 pipeline by ONE persistent cooperative launch per RK
+ * stage (phase A of every box's elements, a grid barrier, phase B), a step
+ * replayed as a CUDA graph. Each box agrees with advancing it alone with
+ * od_step to f32 round-off (same stage code; a few values differ in the last
+ * bit where the compiler contracts multiply-adds differently); results are
+ * deterministic and do not depend on the grid size or the graph. No
+ * reference counterpart (the reference runs one box per process).
+ * ------------------------------------------------------------------------ */
+typedef struct od_ensemble od_ensemble;
+
+typedef struct od_box {
+    int nx, ny, nz;
+    double lx, ly, lz;     /* f32 values widened */
+    int flux;              /* OD_FLUX_* */
+    int y_wall;            /* 1 = slip walls in y */
+    double mu, forcing;    /* constant viscosity, rho*u source */
+    double dt;             /* this box's time step (f32 value widened) */
+} od_box;
+
+int od_ensemble_create(const od_box* boxes, int nbox, int device, int fast_math, od_ensemble** out);
+void od_ensemble_destroy(od_ensemble* e);
+size_t od_ensemble_state_bytes(const od_ensemble* e, int box);
+int od_ensemble_set_state(od_ensemble* e, int box, const void* host, size_t bytes);   /* f32 planes */
+int od_ensemble_get_state(od_ensemble* e, int box, void* host, size_t bytes);
+/* n SSP-RK3 steps of every box; waits for completion and reports a timed-out
+ * grid barrier (the bounded wait's error flag) as OD_ERR_CUDA. */
+int od_ensemble_step(od_ensemble* e, int n_steps);
+/* Launch shape: elements per block (2 or 4; 16 threads each), blocks per SM
+ * (<= 0: all that are co-resident), CUDA graph on/off. */
+int od_ensemble_set_shape(od_ensemble* e, int elems_per_block, int blocks_per_sm, int use_graph);
+int od_ensemble_info(const od_ensemble* e, int* elems_per_block, int* blocks_per_sm, int* grid, int* graph);
+/* Autotuner: times every candidate shape for trial_steps steps on the
+ * ensemble itself (states restored afterwards), keeps the fastest; report
+ * (may be null) receives one line per candidate. */
+int od_ensemble_autotune(od_ensemble* e, int trial_steps, char* report, size_t report_len);
+const char* od_ensemble_last_error(const od_ensemble* e);
+void* od_ensemble_stream(od_ensemble* e);
+
+/* BF16 tensor-core GEMM of the closure network (tcgen05, fp32 accumulation
+ * in tensor memory): C[M x N] (+ bias[N]) = A[M x K] * B[N x K]^T, A and B
+ * bf16 row-major in device memory, C fp32. M % 128 == 0, N % 128 == 0,
+ * K % 64 == 0. Synchronous on `stream`. Exposed for tests; the closure uses
+ * the same kernel with fused epilogues. No reference counterpart. */
+int od_gemm_bf16(int M, int N, int K, const void* dA, const void* dB, float* dC, const float* dbias, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned closure (no reference counterpart): a per-element MLP
+ * 896 -> 256 -> 256 -> 256 -> 320 (GELU) whose output, scaled per variable,
+ * is added to the RHS of an under-resolved coarse run. Inputs: 64 points x
+ * (5 conserved + 9 velocity gradients du_i/dx_j) per element, standardised
+ * with per-channel constants. BF16 weights and activations, fp32
+ * accumulation on the tcgen05 tensor cores; fp32 master weights and Adam.
+ * Parameters (flat fp32): W1 [256 x 896], b1 [256], W2 [256 x 256], b2,
+ * W3 [256 x 256], b3, W4 [384 x 256], b4 [384] (rows 320..383 of the last
+ * layer are padding and stay zero). Output column v*64 + p corrects
+ * variable v at point p.
+ * ------------------------------------------------------------------------ */
+typedef struct od_mlp od_mlp;
+int od_mlp_create(int max_rows, int device, od_mlp** out);
+void od_mlp_destroy(od_mlp* m);
+const char* od_mlp_last_error(const od_mlp* m);
+long long od_mlp_param_count(const od_mlp* m);
+int od_mlp_set_params(od_mlp* m, const float* host_params);   /* also resets Adam */
+int od_mlp_get_params(od_mlp* m, float* host_params);
+/* Y [rows x 384] fp32 = network(X [rows x 896] bf16), device pointers, rows % 128 == 0 */
+int od_mlp_forward(od_mlp* m, const void* X, int rows, float* Y);
+/* gradients (host, flat layout) of mean((Y - T)^2) over the first `valid`
+ * rows and 320 columns; X, XT = X^T [896 x rows] bf16, T [rows x 384] fp32 */
+int od_mlp_gradients(od_mlp* m, const void* X, const void* XT, const float* T, int rows, int valid, float* grads,
+                     double* loss);
+/* one Adam step (lr; betas 0.9, 0.999) on the rows `rows_host` of device
+ * pools Xpool [n x 896] bf16 / Tpool [n x 320] bf16; loss = batch MSE */
+int od_mlp_train_step(od_mlp* m, const void* Xpool, const void* Tpool, const long long* rows_host, int batch,
+                      float lr, double* loss);
+/* input standardisation (x - mean) / scale per channel (14) and output scale per variable (5) */
+int od_mlp_set_scaling(od_mlp* m, const float* mean14, const float* scale14, const float* out_scale5);
+/* Attach (m != null) or detach the network to a solver: every RK stage of
+ * od_step then runs phase A, features of the stage's state, the network,
+ * rhs += out_scale * output, phase B. Needs an f32 state. The network must
+ * outlive the attachment. */
+int od_attach_closure(od_ctx* ctx, od_mlp* m);
+
+/* Data kernels on caller-owned device memory, enqueued on `stream`:
+ * L2 projection of a fine state (5 planes, mesh factor*nxc x factor*nyc x
+ * factor*nzc) onto the coarse nxc x nyc x nzc P=3 basis (exact for the
+ * piecewise-cubic fine field) ... */
+int od_project(const void* src, int src_f64, int nxc, int nyc, int nzc, int factor, void* dst, int dst_f64,
+               void* stream);
+/* ... the network's standardised bf16 feature rows [nelem x 896] of a state ... */
+int od_closure_features(const void* state, int u_f64, int nx, int ny, int nz, double lx, double ly, double lz,
+                        const float* mean14, const float* scale14, void* X, void* stream);
+/* ... and an fp32 -> bf16 conversion. */
+int od_f32_to_bf16(const float* a, void* b, long long n, void* stream);
 
 /* FR P=3 operator tables in double, as src/fr_math.rs:107-142 builds them:
  * points[4], D[16] (D[i*4+j] = l'_j(x_i)), extrap_left[4], extrap_right[4],

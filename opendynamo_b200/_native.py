@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libo
 
 OD_FLUX = {"slau2": 0, "ausm+": 1, "rusanov": 2}
 OD_F32, OD_F64 = 0, 1
+OD_VISC_CONSTANT, OD_VISC_SUTHERLAND = 0, 1
 
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "size mismatch", -4: "call out of order", -5: "I/O error",
           -6: "mesh exceeds the no-alloc scratch"}
@@ -23,6 +24,14 @@ EXPORTS = (
     "od_set_state_device", "od_get_state_device", "od_step", "od_rhs", "od_sync", "od_stream",
     "od_launches_per_step", "od_set_launch_shape", "od_set_pipeline_slabs", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
     "od_rhs_noalloc", "od_state_save", "od_state_info", "od_state_load", "od_state_error", "od_run",
+    "od_diagnostics",
+    "od_ensemble_create", "od_ensemble_destroy", "od_ensemble_state_bytes", "od_ensemble_set_state",
+    "od_ensemble_get_state", "od_ensemble_step", "od_ensemble_set_shape", "od_ensemble_info",
+    "od_ensemble_autotune", "od_ensemble_last_error", "od_ensemble_stream",
+    "od_gemm_bf16",
+    "od_mlp_create", "od_mlp_destroy", "od_mlp_last_error", "od_mlp_param_count", "od_mlp_set_params",
+    "od_mlp_get_params", "od_mlp_forward", "od_mlp_gradients", "od_mlp_train_step", "od_mlp_set_scaling",
+    "od_attach_closure", "od_project", "od_closure_features", "od_f32_to_bf16",
 )
 
 
@@ -36,6 +45,7 @@ class OdParams(ctypes.Structure):
         ("mixed", ctypes.c_int), ("fast_math", ctypes.c_int),
         ("mu", ctypes.c_double), ("forcing", ctypes.c_double),
         ("device", ctypes.c_int), ("ref_compat", ctypes.c_int),
+        ("viscosity_model", ctypes.c_int), ("t_ref", ctypes.c_double), ("s_suth", ctypes.c_double),
     ]
 
 
@@ -56,6 +66,15 @@ class OdRunResult(ctypes.Structure):
         ("files_written", ctypes.c_longlong), ("io_errors", ctypes.c_longlong),
         ("rho_min", ctypes.c_float), ("rho_max", ctypes.c_float),
         ("u_min", ctypes.c_float), ("u_max", ctypes.c_float),
+    ]
+
+
+class OdBox(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("flux", ctypes.c_int), ("y_wall", ctypes.c_int),
+        ("mu", ctypes.c_double), ("forcing", ctypes.c_double), ("dt", ctypes.c_double),
     ]
 
 
@@ -106,6 +125,34 @@ def lib() -> ctypes.CDLL:
                                ctypes.POINTER(cd)]),
         "od_state_error": (ctypes.c_char_p, []),
         "od_run": (ci, [P, ctypes.POINTER(OdRunOpts), ctypes.POINTER(OdRunResult), ctypes.c_char_p, sz]),
+        "od_diagnostics": (ci, [vp, vp, vp, sz]),
+        "od_ensemble_create": (ci, [ctypes.POINTER(OdBox), ci, ci, ci, ctypes.POINTER(vp)]),
+        "od_ensemble_destroy": (None, [vp]),
+        "od_ensemble_state_bytes": (sz, [vp, ci]),
+        "od_ensemble_set_state": (ci, [vp, ci, vp, sz]),
+        "od_ensemble_get_state": (ci, [vp, ci, vp, sz]),
+        "od_ensemble_step": (ci, [vp, ci]),
+        "od_ensemble_set_shape": (ci, [vp, ci, ci, ci]),
+        "od_ensemble_info": (ci, [vp, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci),
+                                  ctypes.POINTER(ci)]),
+        "od_ensemble_autotune": (ci, [vp, ci, ctypes.c_char_p, sz]),
+        "od_ensemble_last_error": (ctypes.c_char_p, [vp]),
+        "od_ensemble_stream": (vp, [vp]),
+        "od_gemm_bf16": (ci, [ci, ci, ci, vp, vp, vp, vp, vp]),
+        "od_mlp_create": (ci, [ci, ci, ctypes.POINTER(vp)]),
+        "od_mlp_destroy": (None, [vp]),
+        "od_mlp_last_error": (ctypes.c_char_p, [vp]),
+        "od_mlp_param_count": (ctypes.c_longlong, [vp]),
+        "od_mlp_set_params": (ci, [vp, vp]),
+        "od_mlp_get_params": (ci, [vp, vp]),
+        "od_mlp_forward": (ci, [vp, vp, ci, vp]),
+        "od_mlp_gradients": (ci, [vp, vp, vp, vp, ci, ci, vp, ctypes.POINTER(cd)]),
+        "od_mlp_train_step": (ci, [vp, vp, vp, vp, ci, ctypes.c_float, ctypes.POINTER(cd)]),
+        "od_mlp_set_scaling": (ci, [vp, vp, vp, vp]),
+        "od_attach_closure": (ci, [vp, vp]),
+        "od_project": (ci, [vp, ci, ci, ci, ci, ci, vp, ci, vp]),
+        "od_closure_features": (ci, [vp, ci, ci, ci, ci, cd, cd, cd, vp, vp, vp, vp]),
+        "od_f32_to_bf16": (ci, [vp, vp, ctypes.c_longlong, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

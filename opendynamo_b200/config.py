@@ -8,7 +8,9 @@ As in the reference, ``viscosity_model``, ``mu_ref``, ``t_ref`` and ``s_suth``
 are parsed but do not change the solver (the reference hardcodes
 mu = 1.6e-4 in src/cuda/constants.cuh:42 and never reads them). The
 optional ``[b200]`` table holds this project's extensions; without it the
-physics is the reference's.
+physics is the reference's: ``mu``, ``forcing``, ``precision_form =
+"mixed"``, ``viscosity_model = "sutherland"`` (Sutherland's law with
+[physics] t_ref / s_suth) and ``re_bulk`` (mu = mach_bulk * (ly/2) / re_bulk).
 """
 
 from __future__ import annotations
@@ -89,6 +91,13 @@ class B200Config:
     mu: float = 1.6e-4          # dynamic viscosity (reference constant)
     forcing: float = 1e-3       # rho*u source (reference constant)
     precision_form: str = "reference"   # "reference" | "mixed" (f64 state/RK/pressure, f32 fluxes)
+    viscosity_model: str = "reference"  # "reference" (constant mu) | "sutherland" ([physics] t_ref, s_suth)
+    re_bulk: Optional[float] = None     # if set: mu = mach_bulk * (ly / 2) / re_bulk (bulk Reynolds number)
+
+    def effective_mu(self, mach_bulk: float, ly: float) -> float:
+        if self.re_bulk is None:
+            return self.mu
+        return mach_bulk * (0.5 * ly) / self.re_bulk
 
 
 @dataclasses.dataclass
@@ -157,6 +166,9 @@ def parse_config(data: dict[str, Any]) -> Config:
         raise ConfigError("[io] checkpoint_freq must be a non-negative integer")
     _enum(io.compression, COMPRESSIONS, "compression")
     _enum(b200.precision_form, ("reference", "mixed"), "precision_form")
+    _enum(b200.viscosity_model, ("reference", "sutherland"), "[b200] viscosity_model")
+    if b200.re_bulk is not None and not (isinstance(b200.re_bulk, (int, float)) and b200.re_bulk > 0):
+        raise ConfigError("[b200] re_bulk must be a positive number")
     if b200.precision_form == "mixed" and (precision.u_real != "f64" or precision.compute_real != "f32"):
         raise ConfigError('precision_form = "mixed" needs u_real = "f64" and compute_real = "f32"')
     return Config(mesh, physics, solver, io, precision, b200)

@@ -144,6 +144,8 @@ struct od_ctx {
     std::vector<cudaEvent_t> events;
     size_t ev_used = 0;
     long long n_stages = 0;
+    od::StageHook hook = nullptr;   // learned closure between phase A and phase B
+    void* hook_user = nullptr;
 };
 
 namespace {
@@ -184,6 +186,7 @@ int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, doub
     L.rc = rc;
     L.mu = c->p.mu;
     L.forcing = c->p.forcing;
+    L.suth = c->p.viscosity_model == OD_VISC_SUTHERLAND ? c->p.s_suth / c->p.t_ref : -1.0;
     L.flags = c->round_flags | (u0 ? 1 : 0);
     L.flux = c->p.flux;
     L.epb_a = c->epb_a;
@@ -200,6 +203,26 @@ int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, doub
         c->ev_used += 3;
     }
     const int K = c->slabs;
+    if (c->hook) {
+        // phase A leaves the RHS in c->rhs; the hook corrects it; phase B finishes the stage
+        L.e0 = 0;
+        L.e1 = c->nelem;
+        L.phases = 1;
+        L.ev[0] = tev[0];
+        L.ev[1] = tev[1];
+        L.ev[2] = nullptr;
+        cudaError_t e = c->fns.launch(L, c->stream);
+        if (e == cudaSuccess) e = c->hook(c->hook_user, u_in, c->rhs, c->stream);
+        if (e == cudaSuccess) {
+            L.phases = 2;
+            L.ev[0] = L.ev[1] = nullptr;
+            L.ev[2] = tev[2];
+            e = c->fns.launch(L, c->stream);
+        }
+        if (e != cudaSuccess) return cuda_fail(c, e, "stage launch (closure)");
+        c->n_stages++;
+        return OD_OK;
+    }
     if (K <= 1) {
         L.phases = 3;
         L.e0 = 0;
@@ -269,6 +292,9 @@ void od_default_params(od_params* p) {
     p->fast_math = 1;
     p->mu = 1.6e-4;
     p->forcing = 1e-3;
+    p->viscosity_model = OD_VISC_CONSTANT;
+    p->t_ref = 273.15;
+    p->s_suth = 110.4;
 }
 
 int od_fr_tables(double* out) {
@@ -288,6 +314,9 @@ int od_create(const od_params* p, od_ctx** out) {
     *out = nullptr;
     if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->flux < 0 || p->flux > 2 || !(p->lx > 0) ||
         !(p->ly > 0) || !(p->lz > 0))
+        return OD_ERR_ARG;
+    if (p->viscosity_model != OD_VISC_CONSTANT &&
+        (p->viscosity_model != OD_VISC_SUTHERLAND || !(p->t_ref > 0) || !(p->s_suth >= 0)))
         return OD_ERR_ARG;
     long long nelem = (long long)p->nx * p->ny * p->nz;
     if (nelem * 64 * 5 >= (1LL << 40)) return OD_ERR_ARG;
@@ -472,6 +501,48 @@ int od_rhs(od_ctx* c, void* d_out, size_t bytes) {
         return fail(c, OD_ERR_ARG, "RHS output must not alias the state");
     if (int rc = set_device(c)) return rc;
     return enqueue_stage(c, c->U[0], nullptr, d_out, 0.0, 0.0, 1.0);
+}
+
+int od_diagnostics(od_ctx* c, double* vol6, double* prof, size_t prof_len) {
+    if (!c || !vol6) return OD_ERR_ARG;
+    if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    const size_t nprof = (size_t)c->p.ny * 4 * 8;
+    if (prof && prof_len < nprof) return fail(c, OD_ERR_SIZE, "profile buffer smaller than ny*4*8");
+    if (int rc = set_device(c)) return rc;
+    double* d = nullptr;
+    const size_t bytes = (6 + nprof) * sizeof(double);
+    cudaError_t e = cudaMallocAsync((void**)&d, bytes, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, bytes, c->stream);
+    if (e == cudaSuccess)
+        e = od::launch_diag(c->U[0], c->elem_size == 8, c->p.nx, c->p.ny, c->p.nz, c->p.lx, c->p.ly, c->p.lz,
+                            c->tab, d, prof ? d + 6 : nullptr, c->stream);
+    std::vector<double> h(6 + nprof);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (d) cudaFreeAsync(d, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "diagnostics");
+    std::copy(h.begin(), h.begin() + 6, vol6);
+    if (prof) {
+        const double area = c->p.lx * c->p.lz;
+        for (size_t i = 0; i < nprof; ++i) prof[i] = h[6 + i] / area;
+    }
+    return OD_OK;
+}
+
+int od_attach_closure(od_ctx* c, od_mlp* m) {
+    if (!c) return OD_ERR_ARG;
+    if (!m) {
+        c->hook = nullptr;
+        c->hook_user = nullptr;
+        return OD_OK;
+    }
+    if (!c->rhs) return fail(c, OD_ERR_ARG, "the closure needs an f32 state (the RHS buffer between phases)");
+    if (int rc = set_device(c)) return rc;
+    if (int rc = od::closure_prepare(m, c->p.nx, c->p.ny, c->p.nz, c->p.lx, c->p.ly, c->p.lz, c->elem_size == 8))
+        return fail(c, rc, od_mlp_last_error(m));
+    c->hook = od::closure_stage_hook;
+    c->hook_user = m;
+    return OD_OK;
 }
 
 int od_sync(od_ctx* c) {

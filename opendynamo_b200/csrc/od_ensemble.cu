@@ -1,0 +1,589 @@
+// Ensembles: many independent boxes (own mesh, extents, flux scheme,
+// viscosity, time step) advanced together, f32 pipeline.
+//
+// One persistent cooperative launch per RK stage covers every box: the grid
+// (sized to what is co-resident: blocks per SM x SM count) walks the phase-A
+// tiles of all boxes in contiguous chunks, meets at a grid barrier, then walks
+// the phase-B tiles. The per-element work is the single-box stage code
+// (stage_a_tile / stage_b_tile of od_stage.cuh) with the flux scheme chosen
+// at run time, so every box agrees with advancing it alone with od_step to
+// f32 round-off (the compiler contracts a few multiply-adds differently in
+// this kernel: a handful of values per box differ in the last bit); for a
+// given shape the result is deterministic. A step (three stage launches) is
+// captured once as a CUDA graph and replayed.
+//
+// The grid barrier is a monotonically growing arrival counter: each launch
+// adds exactly gridDim.x arrivals, a block waits for the next multiple. The
+// wait is bounded: after kSpinLimit polls the block sets the error flag and
+// returns without running phase B; the host reports the flag after the step.
+// The cooperative launch guarantees co-residency, so the bound is a guard, not
+// a schedule.
+//
+// The autotuner times each candidate shape (elements per block, blocks per
+// SM) on the ensemble itself for a few steps and keeps the fastest.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/opendynamo.h"
+#include "od_launch.h"
+#include "od_stage.cuh"
+
+namespace od {
+TablesD host_fr_tables();
+}
+
+namespace {
+
+using od::LPE;
+using od::NE;
+using od::NF;
+using od::SlotA;
+using StageA = od::StageAParams<float, float, float>;
+using StageB = od::StageBParams<float, float, float>;
+
+struct GridSync {
+    unsigned long long count;
+    int err;
+    int pad;
+};
+
+constexpr long long kSpinLimit = 1LL << 25;
+
+struct EnsBoxStage {
+    StageA A;
+    StageB B;
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridSync* g) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned long long n = gridDim.x;
+        const unsigned long long old = atomicAdd(&g->count, 1ull);
+        const unsigned long long target = (old / n + 1) * n;
+        int good = 1;
+        for (long long it = 0;; ++it) {
+            if (ld_acquire(&g->count) >= target) break;
+            if (it >= kSpinLimit || *(volatile int*)&g->err) {
+                atomicExch(&g->err, 1);
+                good = 0;
+                break;
+            }
+            __nanosleep(100);
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// box of global tile t (starts: nbox + 1 prefix sums)
+__device__ __forceinline__ int find_box(const long long* starts, int nbox, long long t) {
+    int lo = 0, hi = nbox - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (starts[mid] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class T>
+__device__ __forceinline__ void block_copy(T* dst, const T* src) {
+    static_assert(sizeof(T) % 4 == 0, "word copy");
+    const int n = sizeof(T) / 4;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        reinterpret_cast<int*>(dst)[i] = reinterpret_cast<const int*>(src)[i];
+}
+
+template <class M, int EPB>
+__global__ void __launch_bounds__(LPE * EPB) ensemble_stage_kernel(const EnsBoxStage* __restrict__ boxes, int nbox,
+                                                                   const long long* __restrict__ start_a,
+                                                                   const long long* __restrict__ start_b,
+                                                                   GridSync* sync) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) StageA As;
+    __shared__ __align__(16) StageB Bs;
+    __shared__ int box_s;
+    const long long G = gridDim.x;
+    // phase A: this block's contiguous chunk of all boxes' tiles
+    {
+        const long long total = start_a[nbox];
+        const long long t0 = total * blockIdx.x / G, t1 = total * (blockIdx.x + 1) / G;
+        int cur = -1;
+        for (long long t = t0; t < t1; ++t) {
+            if (threadIdx.x == 0) box_s = find_box(start_a, nbox, t);
+            __syncthreads();
+            const int b = box_s;
+            if (b != cur) {
+                block_copy(&As, &boxes[b].A);
+                cur = b;
+            }
+            __syncthreads();
+            od::stage_a_tile<float, float, float, M, od::kFluxRuntime, EPB>(As, smem_raw, t - start_a[b]);
+        }
+    }
+    if (!grid_barrier(sync)) return;
+    // phase B
+    {
+        const long long total = start_b[nbox];
+        const long long t0 = total * blockIdx.x / G, t1 = total * (blockIdx.x + 1) / G;
+        int cur = -1;
+        for (long long t = t0; t < t1; ++t) {
+            __syncthreads();
+            if (threadIdx.x == 0) box_s = find_box(start_b, nbox, t);
+            __syncthreads();
+            const int b = box_s;
+            if (b != cur) {
+                __syncthreads();
+                block_copy(&Bs, &boxes[b].B);
+                cur = b;
+                __syncthreads();
+            }
+            od::stage_b_tile<float, float, float, EPB, true>(Bs, t - start_b[b]);
+        }
+    }
+}
+
+template <class M, int EPB>
+void* kernel_ptr() {
+    return (void*)ensemble_stage_kernel<M, EPB>;
+}
+
+void* pick_kernel(bool fast, int epb) {
+    if (fast) return epb == 2 ? kernel_ptr<od::MathFast, 2>() : kernel_ptr<od::MathFast, 4>();
+    return epb == 2 ? kernel_ptr<od::MathIeee, 2>() : kernel_ptr<od::MathIeee, 4>();
+}
+
+size_t dyn_smem(int epb) { return sizeof(SlotA<float, float>) * (size_t)epb; }
+
+}  // namespace
+
+struct od_ensemble {
+    std::vector<od_box> box;
+    int device = 0;
+    bool fast = true;
+    cudaStream_t stream = nullptr;
+    int nsm = 0;
+    // device memory
+    void* pool = nullptr;
+    std::vector<float*> U[3];
+    std::vector<float*> rhs, fv;
+    std::vector<long long> nelem;
+    EnsBoxStage* d_stage[3] = {nullptr, nullptr, nullptr};
+    long long* d_start_a = nullptr;  // per EPB choice: rebuilt by set_shape
+    long long* d_start_b = nullptr;
+    GridSync* d_sync = nullptr;
+    // shape
+    int epb = 4, bps = 0, grid = 0;
+    bool use_graph = true, graph_ok = false;
+    cudaGraphExec_t exec = nullptr;
+    std::string err;
+    long long steps_done = 0;
+};
+
+namespace {
+
+int efail(od_ensemble* e, int code, const std::string& m) {
+    if (e) e->err = m;
+    return code;
+}
+
+int ecuda(od_ensemble* e, cudaError_t c, const char* what) {
+    return efail(e, OD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(c));
+}
+
+// RK stage parameters of every box for the current shape
+int build_stage_params(od_ensemble* E) {
+    const od::TablesD tab = od::host_fr_tables();
+    const int nb = (int)E->box.size();
+    std::vector<EnsBoxStage> h(nb);
+    std::vector<long long> sa(nb + 1, 0), sb(nb + 1, 0);
+    for (int b = 0; b < nb; ++b) {
+        sa[b + 1] = sa[b] + (E->nelem[b] + E->epb - 1) / E->epb;
+        sb[b + 1] = sb[b] + (E->nelem[b] + E->epb - 1) / E->epb;
+    }
+    for (int s = 0; s < 3; ++s) {
+        for (int b = 0; b < nb; ++b) {
+            const od_box& x = E->box[b];
+            StageA& A = h[b].A;
+            std::memset(&A, 0, sizeof A);
+            const float dt = (float)x.dt;
+            // stage coefficients in f32 (od_step, src/solver.rs:275-316)
+            const float ra[3] = {0.0f, 0.75f, (float)(1.0 / 3.0)};
+            const float rb[3] = {1.0f, 0.25f, (float)(2.0 / 3.0)};
+            const float rc[3] = {dt, 0.25f * dt, (float)(2.0 / 3.0) * dt};
+            float* in[3] = {E->U[0][b], E->U[1][b], E->U[2][b]};
+            float* out[3] = {E->U[1][b], E->U[2][b], E->U[0][b]};
+            A.u_in = in[s];
+            A.u0 = s == 0 ? nullptr : E->U[0][b];
+            A.u_out = E->rhs[b];
+            A.fv = E->fv[b];
+            A.fi = E->fv[b] + E->nelem[b] * 6 * 4 * NF;
+            A.m.nx = x.nx;
+            A.m.ny = x.ny;
+            A.m.nz = x.nz;
+            A.m.y_wall = x.y_wall;
+            A.m.nelem = E->nelem[b];
+            A.m.npts = E->nelem[b] * NE;
+            for (int i = 0; i < 16; ++i) A.tp.D[i] = A.tc.D[i] = (float)tab.D[i];
+            for (int i = 0; i < 4; ++i) {
+                A.tp.eL[i] = A.tc.eL[i] = (float)tab.eL[i];
+                A.tp.eR[i] = A.tc.eR[i] = (float)tab.eR[i];
+                A.tp.gL[i] = A.tc.gL[i] = (float)tab.gL[i];
+                A.tp.gR[i] = A.tc.gR[i] = (float)tab.gR[i];
+            }
+            const double L3[3] = {x.lx, x.ly, x.lz};
+            const int n3[3] = {x.nx, x.ny, x.nz};
+            for (int d = 0; d < 3; ++d) A.jac[d] = 2.0f / ((float)L3[d] / (float)n3[d]);
+            A.ra = ra[s];
+            A.rb = rb[s];
+            A.rc = rc[s];
+            A.mu = (float)x.mu;
+            A.forcing = (float)x.forcing;
+            A.suth = -1.0f;
+            A.flags = od::kDeferRK | (s == 0 ? 0 : od::kHasU0);
+            A.flux = x.flux;
+            A.e0 = 0;
+            A.e1 = E->nelem[b];
+            StageB& B = h[b].B;
+            std::memset(&B, 0, sizeof B);
+            B.u_out = out[s];
+            B.rhs = E->rhs[b];
+            B.u_in = in[s];
+            B.u0 = A.u0;
+            B.fv = A.fv;
+            B.fi = A.fi;
+            B.m = A.m;
+            B.tc = A.tc;
+            for (int d = 0; d < 3; ++d) B.jac[d] = A.jac[d];
+            B.ra = A.ra;
+            B.rb = A.rb;
+            B.rc = A.rc;
+            B.flags = A.flags;
+            B.e0 = 0;
+            B.e1 = E->nelem[b];
+        }
+        cudaError_t c = cudaMemcpy(E->d_stage[s], h.data(), sizeof(EnsBoxStage) * nb, cudaMemcpyHostToDevice);
+        if (c != cudaSuccess) return ecuda(E, c, "stage parameters");
+    }
+    cudaError_t c = cudaMemcpy(E->d_start_a, sa.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice);
+    if (c == cudaSuccess) c = cudaMemcpy(E->d_start_b, sb.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice);
+    if (c != cudaSuccess) return ecuda(E, c, "tile tables");
+    return OD_OK;
+}
+
+cudaError_t launch_stage(od_ensemble* E, int s) {
+    void* fn = pick_kernel(E->fast, E->epb);
+    int nbox = (int)E->box.size();
+    void* args[] = {(void*)&E->d_stage[s], (void*)&nbox, (void*)&E->d_start_a, (void*)&E->d_start_b,
+                    (void*)&E->d_sync};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)E->grid);
+    cfg.blockDim = dim3((unsigned)(LPE * E->epb));
+    cfg.dynamicSmemBytes = dyn_smem(E->epb);
+    cfg.stream = E->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+void drop_graph(od_ensemble* E) {
+    if (E->exec) cudaGraphExecDestroy(E->exec);
+    E->exec = nullptr;
+    E->graph_ok = false;
+}
+
+// set the launch shape; blocks_per_sm <= 0 = as many as are co-resident
+int apply_shape(od_ensemble* E, int epb, int bps, bool use_graph) {
+    if (epb != 2 && epb != 4) return efail(E, OD_ERR_ARG, "elements per block must be 2 or 4");
+    void* fn = pick_kernel(E->fast, epb);
+    cudaError_t c = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem(epb));
+    if (c != cudaSuccess) return ecuda(E, c, "cudaFuncSetAttribute");
+    int maxb = 0;
+    c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, LPE * epb, dyn_smem(epb));
+    if (c != cudaSuccess) return ecuda(E, c, "occupancy");
+    if (maxb <= 0) return efail(E, OD_ERR_CUDA, "ensemble kernel cannot be resident");
+    if (bps <= 0 || bps > maxb) bps = maxb;
+    drop_graph(E);
+    const bool epb_changed = epb != E->epb;
+    E->epb = epb;
+    E->bps = bps;
+    E->grid = bps * E->nsm;
+    E->use_graph = use_graph;
+    if (epb_changed || !E->d_stage[0]) {
+        if (int rc = build_stage_params(E)) return rc;
+    }
+    // a new grid size restarts the arrival counter
+    c = cudaMemsetAsync(E->d_sync, 0, sizeof(GridSync), E->stream);
+    if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
+    if (c != cudaSuccess) return ecuda(E, c, "barrier reset");
+    if (use_graph) {
+        cudaGraph_t g = nullptr;
+        c = cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal);
+        if (c == cudaSuccess) {
+            cudaError_t lc = cudaSuccess;
+            for (int s = 0; s < 3 && lc == cudaSuccess; ++s) lc = launch_stage(E, s);
+            c = cudaStreamEndCapture(E->stream, &g);
+            if (lc != cudaSuccess) c = lc;
+        }
+        if (c == cudaSuccess) c = cudaGraphInstantiate(&E->exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (c != cudaSuccess) {
+            cudaGetLastError();
+            E->exec = nullptr;
+            E->graph_ok = false;  // direct launches instead
+        } else {
+            E->graph_ok = true;
+        }
+    }
+    return OD_OK;
+}
+
+int enqueue_steps(od_ensemble* E, int n) {
+    for (int i = 0; i < n; ++i) {
+        cudaError_t c;
+        if (E->graph_ok) {
+            c = cudaGraphLaunch(E->exec, E->stream);
+        } else {
+            c = cudaSuccess;
+            for (int s = 0; s < 3 && c == cudaSuccess; ++s) c = launch_stage(E, s);
+        }
+        if (c != cudaSuccess) return ecuda(E, c, "ensemble step");
+    }
+    E->steps_done += n;
+    return OD_OK;
+}
+
+int check_sync_flag(od_ensemble* E) {
+    GridSync h;
+    cudaError_t c = cudaMemcpyAsync(&h, E->d_sync, sizeof h, cudaMemcpyDeviceToHost, E->stream);
+    if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
+    if (c != cudaSuccess) return ecuda(E, c, "ensemble step");
+    if (h.err) return efail(E, OD_ERR_CUDA, "ensemble grid barrier timed out (blocks not co-resident)");
+    return OD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int od_ensemble_create(const od_box* boxes, int nbox, int device, int fast_math, od_ensemble** out) {
+    if (!boxes || nbox <= 0 || !out) return OD_ERR_ARG;
+    *out = nullptr;
+    for (int b = 0; b < nbox; ++b) {
+        const od_box& x = boxes[b];
+        if (x.nx <= 0 || x.ny <= 0 || x.nz <= 0 || !(x.lx > 0) || !(x.ly > 0) || !(x.lz > 0) || x.flux < 0 ||
+            x.flux > 2 || !(x.dt > 0) || !(x.mu >= 0))
+            return OD_ERR_ARG;
+    }
+    od_ensemble* E = new od_ensemble();
+    E->box.assign(boxes, boxes + nbox);
+    E->device = device;
+    E->fast = fast_math != 0;
+    cudaError_t c = cudaSetDevice(device);
+    if (c == cudaSuccess) c = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
+    if (c == cudaSuccess) c = cudaDeviceGetAttribute(&E->nsm, cudaDevAttrMultiProcessorCount, device);
+    int coop = 0;
+    if (c == cudaSuccess) c = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (c != cudaSuccess || !coop) {
+        *out = E;
+        return c != cudaSuccess ? ecuda(E, c, "device setup") : efail(E, OD_ERR_CUDA, "no cooperative launch");
+    }
+    size_t total = 0;
+    std::vector<size_t> off(nbox);
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    for (int b = 0; b < nbox; ++b) {
+        const long long ne = (long long)boxes[b].nx * boxes[b].ny * boxes[b].nz;
+        E->nelem.push_back(ne);
+        off[b] = total;
+        const size_t st = (size_t)ne * NE * 5 * sizeof(float);
+        total += 4 * align(st) + align((size_t)ne * (6 * 4 + 3 * 5) * NF * sizeof(float));
+    }
+    c = cudaMalloc(&E->pool, total);
+    if (c == cudaSuccess) c = cudaMemset(E->pool, 0, total);
+    for (int s = 0; s < 3 && c == cudaSuccess; ++s) c = cudaMalloc(&E->d_stage[s], sizeof(EnsBoxStage) * nbox);
+    if (c == cudaSuccess) c = cudaMalloc(&E->d_start_a, sizeof(long long) * (nbox + 1));
+    if (c == cudaSuccess) c = cudaMalloc(&E->d_start_b, sizeof(long long) * (nbox + 1));
+    if (c == cudaSuccess) c = cudaMalloc(&E->d_sync, sizeof(GridSync));
+    if (c != cudaSuccess) {
+        *out = E;
+        return ecuda(E, c, "allocation");
+    }
+    for (int b = 0; b < nbox; ++b) {
+        char* p = (char*)E->pool + off[b];
+        const size_t st = align((size_t)E->nelem[b] * NE * 5 * sizeof(float));
+        for (int k = 0; k < 3; ++k) E->U[k].push_back((float*)(p + k * st));
+        E->rhs.push_back((float*)(p + 3 * st));
+        E->fv.push_back((float*)(p + 4 * st));
+    }
+    *out = E;
+    E->epb = 0;  // forces the parameter build
+    return apply_shape(E, 4, 0, true);
+}
+
+void od_ensemble_destroy(od_ensemble* E) {
+    if (!E) return;
+    cudaSetDevice(E->device);
+    drop_graph(E);
+    if (E->stream) cudaStreamSynchronize(E->stream);
+    for (int s = 0; s < 3; ++s)
+        if (E->d_stage[s]) cudaFree(E->d_stage[s]);
+    if (E->d_start_a) cudaFree(E->d_start_a);
+    if (E->d_start_b) cudaFree(E->d_start_b);
+    if (E->d_sync) cudaFree(E->d_sync);
+    if (E->pool) cudaFree(E->pool);
+    if (E->stream) cudaStreamDestroy(E->stream);
+    delete E;
+}
+
+size_t od_ensemble_state_bytes(const od_ensemble* E, int b) {
+    if (!E || b < 0 || b >= (int)E->box.size()) return 0;
+    return (size_t)E->nelem[b] * NE * 5 * sizeof(float);
+}
+
+int od_ensemble_set_state(od_ensemble* E, int b, const void* host, size_t bytes) {
+    if (!E || !host || b < 0 || b >= (int)E->box.size()) return OD_ERR_ARG;
+    if (bytes != od_ensemble_state_bytes(E, b)) return efail(E, OD_ERR_SIZE, "state size does not match the box");
+    cudaSetDevice(E->device);
+    cudaError_t c = cudaMemcpyAsync(E->U[0][b], host, bytes, cudaMemcpyHostToDevice, E->stream);
+    if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
+    if (c != cudaSuccess) return ecuda(E, c, "set state");
+    return OD_OK;
+}
+
+int od_ensemble_get_state(od_ensemble* E, int b, void* host, size_t bytes) {
+    if (!E || !host || b < 0 || b >= (int)E->box.size()) return OD_ERR_ARG;
+    if (bytes != od_ensemble_state_bytes(E, b)) return efail(E, OD_ERR_SIZE, "state size does not match the box");
+    cudaSetDevice(E->device);
+    cudaError_t c = cudaMemcpyAsync(host, E->U[0][b], bytes, cudaMemcpyDeviceToHost, E->stream);
+    if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
+    if (c != cudaSuccess) return ecuda(E, c, "get state");
+    return OD_OK;
+}
+
+int od_ensemble_step(od_ensemble* E, int n) {
+    if (!E || n < 0) return OD_ERR_ARG;
+    cudaSetDevice(E->device);
+    if (int rc = enqueue_steps(E, n)) return rc;
+    return check_sync_flag(E);
+}
+
+int od_ensemble_set_shape(od_ensemble* E, int epb, int blocks_per_sm, int use_graph) {
+    if (!E) return OD_ERR_ARG;
+    cudaSetDevice(E->device);
+    return apply_shape(E, epb, blocks_per_sm, use_graph != 0);
+}
+
+int od_ensemble_info(const od_ensemble* E, int* epb, int* blocks_per_sm, int* grid, int* graph) {
+    if (!E) return OD_ERR_ARG;
+    if (epb) *epb = E->epb;
+    if (blocks_per_sm) *blocks_per_sm = E->bps;
+    if (grid) *grid = E->grid;
+    if (graph) *graph = E->graph_ok ? 1 : 0;
+    return OD_OK;
+}
+
+// Times every candidate shape for trial_steps steps (after one warm-up step)
+// on a scratch copy of the states, keeps the fastest and restores the states.
+int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t report_len) {
+    if (!E || trial_steps <= 0) return OD_ERR_ARG;
+    cudaSetDevice(E->device);
+    const int nb = (int)E->box.size();
+    std::vector<void*> save(nb, nullptr);
+    cudaError_t c = cudaSuccess;
+    for (int b = 0; b < nb && c == cudaSuccess; ++b) {
+        c = cudaMalloc(&save[b], od_ensemble_state_bytes(E, b));
+        if (c == cudaSuccess)
+            c = cudaMemcpyAsync(save[b], E->U[0][b], od_ensemble_state_bytes(E, b), cudaMemcpyDeviceToDevice,
+                                E->stream);
+    }
+    if (c != cudaSuccess) {
+        for (void* p : save)
+            if (p) cudaFree(p);
+        return ecuda(E, c, "autotune scratch");
+    }
+    std::string rep;
+    double best = 1e30;
+    int best_epb = 4, best_bps = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = OD_OK;
+    for (int epb : {2, 4}) {
+        void* fn = pick_kernel(E->fast, epb);
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem(epb));
+        int maxb = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, LPE * epb, dyn_smem(epb));
+        std::vector<int> cands;
+        for (int b = maxb; b >= 1; b = b > 2 ? b * 3 / 4 : b - 1) cands.push_back(b);
+        for (int bps : cands) {
+            if ((rc = apply_shape(E, epb, bps, true))) break;
+            if ((rc = enqueue_steps(E, 1))) break;
+            cudaEventRecord(e0, E->stream);
+            if ((rc = enqueue_steps(E, trial_steps))) break;
+            cudaEventRecord(e1, E->stream);
+            if ((rc = check_sync_flag(E))) break;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            char line[128];
+            std::snprintf(line, sizeof line, "epb=%d blocks/SM=%d grid=%d graph=%d: %.4f ms/step\n", epb, bps,
+                          E->grid, E->graph_ok ? 1 : 0, ms / trial_steps);
+            rep += line;
+            if (ms < best) {
+                best = ms;
+                best_epb = epb;
+                best_bps = bps;
+            }
+            // restore the states between trials
+            for (int b = 0; b < nb; ++b)
+                cudaMemcpyAsync(E->U[0][b], save[b], od_ensemble_state_bytes(E, b), cudaMemcpyDeviceToDevice,
+                                E->stream);
+        }
+        if (rc) break;
+    }
+    for (int b = 0; b < nb; ++b) {
+        cudaMemcpyAsync(E->U[0][b], save[b], od_ensemble_state_bytes(E, b), cudaMemcpyDeviceToDevice, E->stream);
+    }
+    cudaStreamSynchronize(E->stream);
+    for (void* p : save) cudaFree(p);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    E->steps_done = 0;
+    rc = apply_shape(E, best_epb, best_bps, true);
+    char line[128];
+    std::snprintf(line, sizeof line, "chosen: epb=%d blocks/SM=%d\n", best_epb, best_bps);
+    rep += line;
+    if (report && report_len) {
+        std::strncpy(report, rep.c_str(), report_len - 1);
+        report[report_len - 1] = 0;
+    }
+    return rc;
+}
+
+const char* od_ensemble_last_error(const od_ensemble* E) { return E ? E->err.c_str() : ""; }
+
+void* od_ensemble_stream(od_ensemble* E) { return E ? (void*)E->stream : nullptr; }
+
+}  // extern "C"

@@ -33,6 +33,7 @@ struct StageLaunch {
     double jac[3];       // already evaluated in the compute type
     double ra, rb, rc;   // already evaluated in the state-arithmetic type
     double mu, forcing;
+    double suth;            // Sutherland S = s_suth / t_ref; < 0: constant mu
     int flags;           // kHasU0 | kRoundQ | kRoundRhs
     int flux;            // 0 slau2, 1 ausm+, 2 rusanov
     int epb_a, epb_b;    // elements per block of phase A / phase B
@@ -50,6 +51,24 @@ enum Combo : int {
     kU32C64 = 3,   // float / double / double
     kMixed = 4,    // double / double / float  (precision form: f64 state, RK and pressure; f32 fluxes)
 };
+
+// Work run between phase A and phase B of every RK stage (the learned
+// closure): reads the stage's input state, may modify the RHS buffer.
+using StageHook = cudaError_t (*)(void* user, const void* u_in, void* rhs, cudaStream_t s);
+
+}  // namespace od
+
+struct od_mlp;
+
+namespace od {
+
+// the learned closure's hook and its per-mesh preparation (od_closure.cu)
+cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStream_t s);
+int closure_prepare(od_mlp* m, int nx, int ny, int nz, double lx, double ly, double lz, bool f64);
+
+// Diagnostics (od_diag.cu): accumulates into d_vol6 / d_prof (zeroed by the caller).
+cudaError_t launch_diag(const void* u, bool u_f64, int nx, int ny, int nz, double lx, double ly, double lz,
+                        const TablesD& tab, double* d_vol6, double* d_prof, cudaStream_t s);
 
 cudaError_t launch_stage_f32(const StageLaunch& L, cudaStream_t s);
 cudaError_t launch_stage_f64(const StageLaunch& L, cudaStream_t s);

@@ -37,6 +37,15 @@ cudaError_t launch_a_epb(const StageAParams<S, P, C>& A, long long nelem, int ep
 
 template <class S, class P, class C, class M>
 cudaError_t launch_a_flux(const StageAParams<S, P, C>& A, int flux, long long nelem, int epb, cudaStream_t s) {
+    if (A.suth >= (C)0) {
+        // Sutherland variant: 4 elements per block only
+        using MS = WithSutherland<M>;
+        switch (flux) {
+            case kSlau2: return launch_a<S, P, C, MS, kSlau2, 4>(A, nelem, s);
+            case kAusmPlus: return launch_a<S, P, C, MS, kAusmPlus, 4>(A, nelem, s);
+            default: return launch_a<S, P, C, MS, kRusanov, 4>(A, nelem, s);
+        }
+    }
     switch (flux) {
         case kSlau2: return launch_a_epb<S, P, C, M, kSlau2>(A, nelem, epb, s);
         case kAusmPlus: return launch_a_epb<S, P, C, M, kAusmPlus>(A, nelem, epb, s);
@@ -78,6 +87,8 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.rc = (P)L.rc;
     A.mu = (C)L.mu;
     A.forcing = (C)L.forcing;
+    A.suth = (C)L.suth;
+    A.flux = L.flux;
     A.flags = L.flags | (L.rhs ? kDeferRK : 0);
     A.e0 = L.e0;
     A.e1 = L.e1;
@@ -128,6 +139,9 @@ cudaError_t prepare_flux() {
     cudaError_t e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, M, FLUX, 2>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(sizeof(SlotA<P, C>) * 2));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(stage_a_kernel<S, P, C, WithSutherland<M>, FLUX, 4>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(SlotA<P, C>) * 4));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(stage_a_kernel<S, P, C, M, FLUX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(sizeof(SlotA<P, C>) * 4));

@@ -1,0 +1,274 @@
+// BF16 tensor-core GEMM for the learned closure on sm_100a (tcgen05 + TMEM).
+//
+//   C[M x N] = A[M x K] * B[N x K]^T     A, B: bf16, row-major, K contiguous
+//                                        accumulation: fp32 in tensor memory
+//
+// One CTA computes a 128 x NT tile (NT = 128 or 256) with 128 threads:
+//   - all threads stage 128 x 64 (A) and NT x 64 (B) bf16 blocks into shared
+//     memory with 16-byte cp.async copies, two stages deep, in the canonical
+//     no-swizzle K-major layout of the tensor cores: 8 x 16-byte core
+//     matrices, the two K halves of an MMA 128 B apart (LBO), 8-row groups
+//     1024 B apart (SBO);
+//   - thread 0 issues tcgen05.mma (kind::f16, M = 128, N = NT, K = 16) four
+//     times per 64-wide block into the TMEM accumulator and commits them to
+//     the stage's mbarrier, so the copy of block k+1 overlaps the MMAs of k;
+//   - the epilogue reads the accumulator with tcgen05.ld (warp w owns rows
+//     32w..32w+31, one row per thread) and applies one of the closure's
+//     fused epilogues (bias, GELU, GELU', transposed copies, fp32 store).
+// Every mbarrier wait is bounded: past the limit the CTA records an error
+// and skips the rest, then frees its tensor memory.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace od {
+namespace mlp {
+
+constexpr int BM = 128;        // rows per CTA tile
+constexpr int BK = 64;         // K per pipeline stage
+constexpr int STAGES = 2;
+constexpr long long kWaitLimit = 1LL << 26;
+
+enum Epi : int {
+    kStoreF32 = 0,     // C (+ bias) -> fp32 [M x N] (ldc = N)
+    kBiasGelu = 1,     // z = C + bias -> z fp32, gelu(z) -> bf16 [M x N] and bf16 transpose [N x M]
+    kGeluGrad = 2,     // dz = C * gelu'(z_in) -> bf16 [M x N] and bf16 transpose [N x M]
+};
+
+struct GemmArgs {
+    const __nv_bfloat16* A;   // [M x K]
+    const __nv_bfloat16* B;   // [N x K]
+    int M, N, K;
+    const float* bias;        // [N] or null
+    float* out_f32;           // kStoreF32: C; kBiasGelu: z
+    __nv_bfloat16* out_bf;    // kBiasGelu: gelu(z); kGeluGrad: dz
+    __nv_bfloat16* out_bfT;   // transposed copy ([N x M]) or null
+    const float* z_in;        // kGeluGrad: the layer's pre-activation [M x N]
+    int* err;                 // set to 1 when a bounded wait gives up
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= 1ull << 46;  // descriptor version of sm_100
+    // base offset 0, leading-byte-offset mode 0, layout type 0 (no swizzle)
+    return d;
+}
+
+// kind::f16 instruction descriptor: bf16 x bf16 -> f32, both K-major
+__host__ __device__ constexpr uint32_t instr_desc(int m, int n) {
+    return (1u << 4)                       // D format f32
+           | (1u << 7)                     // A format bf16
+           | (1u << 10)                    // B format bf16
+           | ((uint32_t)(n >> 3) << 17)    // N / 8
+           | ((uint32_t)(m >> 4) << 24);   // M / 16
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+    const float pdf = 0.3989422804014327f * expf(-0.5f * z * z);
+    return cdf + z * pdf;
+}
+
+// smem offset of (row r, 16-byte K chunk kc) inside a tile
+__device__ __forceinline__ uint32_t tile_off(int r, int kc) {
+    return (uint32_t)((r >> 3) * 1024 + kc * 128 + (r & 7) * 16);
+}
+
+template <int NT>
+struct Smem {
+    alignas(1024) unsigned char a[STAGES][BM * BK * 2];
+    alignas(1024) unsigned char b[STAGES][NT * BK * 2];
+    alignas(8) unsigned long long bar[STAGES];
+    alignas(8) unsigned long long done_bar;
+    uint32_t tmem_base;
+    int failed;
+};
+
+template <int NT>
+__device__ __forceinline__ void load_stage(const GemmArgs& g, Smem<NT>& s, int st, int m0, int n0, int kb) {
+    const int t = threadIdx.x;
+    const int k0 = kb * BK;
+    // A: 128 rows x 8 chunks; 8 consecutive threads cover rows r..r+7 of one chunk
+#pragma unroll
+    for (int i = 0; i < (BM * 8) / 128; ++i) {
+        const int c = t + 128 * i;
+        const int r = (c & 7) + 8 * (c >> 6);
+        const int kc = (c >> 3) & 7;
+        cp_async16(smem_addr(s.a[st]) + tile_off(r, kc), g.A + (size_t)(m0 + r) * g.K + k0 + kc * 8);
+    }
+#pragma unroll
+    for (int i = 0; i < (NT * 8) / 128; ++i) {
+        const int c = t + 128 * i;
+        const int r = (c & 7) + 8 * (c >> 6);
+        const int kc = (c >> 3) & 7;
+        cp_async16(smem_addr(s.b[st]) + tile_off(r, kc), g.B + (size_t)(n0 + r) * g.K + k0 + kc * 8);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int NT, int EPI>
+__global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned view of the dynamic shared memory
+    Smem<NT>& s = *reinterpret_cast<Smem<NT>*>(
+        smem_raw + ((1024 - (smem_addr(smem_raw) & 1023)) & 1023));
+    const int t = threadIdx.x;
+    const int warp = t >> 5;
+    const int m0 = blockIdx.x * BM;
+    const int n0 = blockIdx.y * NT;
+    const int KB = g.K / BK;
+    constexpr uint32_t kCols = NT;  // fp32 accumulator: one column per N
+
+    if (t == 0) {
+        for (int i = 0; i < STAGES; ++i) mbar_init(smem_addr(&s.bar[i]), 1);
+        mbar_init(smem_addr(&s.done_bar), 1);
+        s.failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s.tmem_base)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s.tmem_base;
+    const uint32_t idesc = instr_desc(BM, NT);
+
+    load_stage<NT>(g, s, 0, m0, n0, 0);
+    for (int kb = 0; kb < KB; ++kb) {
+        const int st = kb % STAGES;
+        // block kb has landed in stage st
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (t == 0 && !s.failed) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(s.a[st]), b0 = smem_addr(s.b[st]);
+#pragma unroll
+            for (int k = 0; k < BK / 16; ++k) {
+                const uint64_t ad = smem_desc(a0 + k * 256, 128, 1024);
+                const uint64_t bd = smem_desc(b0 + k * 256, 128, 1024);
+                const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&s.bar[st]))
+                         : "memory");
+        }
+        // prefetch block kb+1 into the other stage once the MMAs that read it (block kb-1) are done
+        if (kb + 1 < KB) {
+            const int nst = (kb + 1) % STAGES;
+            if (kb >= 1) {
+                // completion number (kb-1)/STAGES of bar[nst]
+                const uint32_t parity = (uint32_t)(((kb - 1) / STAGES) & 1);
+                if (!mbar_wait(smem_addr(&s.bar[nst]), parity)) {
+                    s.failed = 1;
+                    if (g.err) atomicExch(g.err, 1);
+                }
+            }
+            __syncthreads();
+            if (!s.failed) load_stage<NT>(g, s, nst, m0, n0, kb + 1);
+        }
+    }
+    // all MMAs done: commit once more on the final barrier
+    if (t == 0 && !s.failed) {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&s.done_bar))
+                     : "memory");
+    }
+    __syncthreads();
+    bool ok = !s.failed;
+    if (ok && !mbar_wait(smem_addr(&s.done_bar), 0)) {
+        ok = false;
+        if (g.err) atomicExch(g.err, 1);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        const int row = m0 + warp * 32 + (t & 31);
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(lane_base + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int n = n0 + c0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                float v = __uint_as_float(r[j]);
+                const size_t idx = (size_t)row * g.N + n + j;
+                if constexpr (EPI == kStoreF32) {
+                    if (g.bias) v += g.bias[n + j];
+                    g.out_f32[idx] = v;
+                } else if constexpr (EPI == kBiasGelu) {
+                    v += g.bias[n + j];
+                    g.out_f32[idx] = v;
+                    const __nv_bfloat16 a = __float2bfloat16_rn(gelu(v));
+                    g.out_bf[idx] = a;
+                    if (g.out_bfT) g.out_bfT[(size_t)(n + j) * g.M + row] = a;
+                } else {
+                    const __nv_bfloat16 d = __float2bfloat16_rn(v * gelu_grad(g.z_in[idx]));
+                    g.out_bf[idx] = d;
+                    if (g.out_bfT) g.out_bfT[(size_t)(n + j) * g.M + row] = d;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+    }
+}
+
+template <int NT>
+constexpr size_t gemm_smem_bytes() {
+    return sizeof(Smem<NT>) + 1024;
+}
+
+}  // namespace mlp
+}  // namespace od

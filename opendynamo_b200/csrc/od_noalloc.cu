@@ -49,6 +49,9 @@ extern "C" int od_rhs_noalloc(const od_params* p, const void* d_state, void* d_r
     if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->flux < 0 || p->flux > 2 || !(p->lx > 0) || !(p->ly > 0) ||
         !(p->lz > 0) || p->device < 0 || p->device >= kMaxDevices)
         return OD_ERR_ARG;
+    if (p->viscosity_model != OD_VISC_CONSTANT &&
+        (p->viscosity_model != OD_VISC_SUTHERLAND || !(p->t_ref > 0) || !(p->s_suth >= 0)))
+        return OD_ERR_ARG;
     od::Combo combo;
     if (p->mixed) {
         if (p->u_real != OD_F64 || p->compute_real != OD_F32) return OD_ERR_ARG;
@@ -123,6 +126,7 @@ extern "C" int od_rhs_noalloc(const od_params* p, const void* d_state, void* d_r
     L.rc = 1.0;
     L.mu = p->mu;
     L.forcing = p->forcing;
+    L.suth = p->viscosity_model == OD_VISC_SUTHERLAND ? p->s_suth / p->t_ref : -1.0;
     int flags = 0;
     if (c_double) {
         if (p->q_real == OD_F32) flags |= od::kRoundQ;

@@ -26,6 +26,7 @@ enum Flux : int { kSlau2 = 0, kAusmPlus = 1, kRusanov = 2 };
 // sqrt.approx, ~1-2 ulp), the arithmetic of the reference's default
 // --use_fast_math build; f64 operands stay IEEE (fast math does not touch them).
 struct MathIeee {
+    static constexpr bool kSutherland = false;
     template <class T>
     static __device__ __forceinline__ T rcp(T x) { return (T)1.0 / x; }
     template <class T>
@@ -35,6 +36,7 @@ struct MathIeee {
 };
 
 struct MathFast {
+    static constexpr bool kSutherland = false;
     template <class T>
     static __device__ __forceinline__ T rcp(T x) {
         if constexpr (sizeof(T) == 4) {
@@ -60,6 +62,13 @@ struct MathFast {
             return ::sqrt(x);
         }
     }
+};
+
+// A math policy with Sutherland's law switched on (a separate kernel variant,
+// so the constant-viscosity kernels carry no trace of it).
+template <class Base>
+struct WithSutherland : Base {
+    static constexpr bool kSutherland = true;
 };
 
 template <class C>
@@ -136,6 +145,22 @@ __device__ __forceinline__ void euler_flux_dyn(const FaceState<C>& s, int d, C* 
 template <class M, class C>
 __device__ __forceinline__ C sound_speed(C p, C r) {
     return M::sqrt(cmax((C)0.0, M::div(Gas<C>::gamma() * p, cmax((C)1e-7, r))));
+}
+
+// Dynamic viscosity at a point. Policies without kSutherland: constant mu
+// (the reference's MU_REF, src/cuda/constants.cuh:42). Otherwise Sutherland's law
+//   mu = mu_ref * T^(3/2) * (1 + S) / (T + S),
+// T = gamma * p / rho the temperature in units of the reference temperature
+// (rho = 1, c = 1 there) and S = s_suth / t_ref (config.toml [physics]).
+// An extension: the reference parses viscosity_model but no kernel reads it.
+template <class M, class C>
+__device__ __forceinline__ C viscosity(C mu, C suth, const FaceState<C>& s) {
+    if constexpr (!M::kSutherland) {
+        return mu;
+    } else {
+        const C T = Gas<C>::gamma() * s.p * s.ir;
+        return mu * T * M::sqrt(T) * M::div((C)1.0 + suth, T + suth);
+    }
 }
 
 // Viscous flux along axis D at a face point from the state and the
@@ -296,6 +321,19 @@ __device__ __forceinline__ void interface_flux(const FaceState<C>& L, const Face
     if constexpr (FLUX == kSlau2)
         slau2<M, D>(L, R, f);
     else if constexpr (FLUX == kAusmPlus)
+        ausm_plus<M, D>(L, R, f);
+    else
+        rusanov<M, D>(L, R, f);
+}
+
+// Scheme chosen at run time (ensembles that mix schemes in one launch).
+constexpr int kFluxRuntime = -1;
+
+template <class M, int D, class C>
+__device__ __forceinline__ void interface_flux_rt(int flux, const FaceState<C>& L, const FaceState<C>& R, C* f) {
+    if (flux == kSlau2)
+        slau2<M, D>(L, R, f);
+    else if (flux == kAusmPlus)
         ausm_plus<M, D>(L, R, f);
     else
         rusanov<M, D>(L, R, f);

@@ -208,7 +208,9 @@ struct StageAParams {
     C jac[3];
     P ra, rb, rc;
     C mu, forcing;
+    C suth;             // Sutherland S = s_suth / t_ref, < 0: constant mu
     int flags;
+    int flux;           // scheme id, read when the kernel's FLUX is kFluxRuntime
     long long e0, e1;   // element range of this launch
 };
 
@@ -227,7 +229,7 @@ __device__ __forceinline__ void wall_face(const FaceState<C>& so, const C* fe, C
 }
 
 template <class M, int FLUX, int D, class P, class C>
-__device__ __forceinline__ void minus_face(const P* own, const P* nbr, bool wall, C* j, C* fi) {
+__device__ __forceinline__ void minus_face(const P* own, const P* nbr, bool wall, C* j, C* fi, int rflux) {
     C praw;
     FaceState<C> so = make_face_state<M, C, P>(own, praw);
     C fe[NV];
@@ -237,7 +239,10 @@ __device__ __forceinline__ void minus_face(const P* own, const P* nbr, bool wall
         return;
     }
     FaceState<C> sn = make_face_state<M, C, P>(nbr, praw);
-    interface_flux<M, FLUX, D>(sn, so, fi);
+    if constexpr (FLUX == kFluxRuntime)
+        interface_flux_rt<M, D>(rflux, sn, so, fi);
+    else
+        interface_flux<M, FLUX, D>(sn, so, fi);
 #pragma unroll
     for (int v = 0; v < NV; ++v) j[v] = fi[v] - fe[v];
 }
@@ -344,7 +349,7 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
     }
     // inviscid parts at the two faces of this line
     C j0[NV], j1[NV], fi[NV];
-    minus_face<M, FLUX, D, P, C>(oL, nL, nb0 < 0, j0, fi);
+    minus_face<M, FLUX, D, P, C>(oL, nL, nb0 < 0, j0, fi, A.flux);
     plus_face<M, D, P, C>(oR, nb1 < 0, j1);
     if (live && nb0 >= 0) {
         C* out = A.fi + ((e * 3 + D) * NV) * NF + l;
@@ -367,7 +372,7 @@ __device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, Slo
     C praw;
     FaceState<C> s = make_face_state<M, C, P>(qp, praw);
     C fv[NV];
-    viscous_flux<D>(s, praw, gt, A.mu, fv);
+    viscous_flux<D>(s, praw, gt, viscosity<M>(A.mu, A.suth, s), fv);
 #pragma unroll
     for (int v = 0; v < NV; ++v) sm.j[f][v][l] += (C)0.5 * fv[v];
     if (live) {
@@ -450,14 +455,68 @@ __device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, con
     }
 }
 
+// P8 of phase A for one live element: RHS = -div + forcing, own-face lifting
+// -(j_L g_L' + j_R g_R') jac, then the RK combination, or (deferred RK) the
+// unrounded RHS + own lift for phase B.
+template <class S, class P, class C>
+__device__ __forceinline__ void stage_a_update(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long ec, int l,
+                                               int swz, const C* divy) {
+    const Mesh& m = A.m;
+    const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
+    const int px = sw(4 * l, swz);
+    const bool defer = (A.flags & kDeferRK) != 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        C dx[4], dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
+        ld4s(&sm.g[10 + v][px], dx);
+        ld4s(&divy[v * NE + px], dy);
+        ld4s(&sm.g[5 + v][px], dz);
+        ld4s(&sm.j[2][v][4 * lk], jy0);
+        ld4s(&sm.j[3][v][4 * lk], jy1);
+        ld4s(&sm.j[4][v][4 * lj], jz0);
+        ld4s(&sm.j[5][v][4 * lj], jz1);
+        const C jx0 = sm.j[0][v][l], jx1 = sm.j[1][v][l];
+        C rt[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            C rvol = -((dx[i] + dy[i]) + dz[i]);
+            if (v == 1) rvol += A.forcing;
+            if constexpr (sizeof(C) == 8) {
+                if (A.flags & kRoundRhs) rvol = (C)(float)rvol;
+            }
+            const C cx = -(jx0 * A.tc.gL[i] * A.jac[0]) - (jx1 * A.tc.gR[i] * A.jac[0]);
+            const C cy = -(jy0[i] * A.tc.gL[lj] * A.jac[1]) - (jy1[i] * A.tc.gR[lj] * A.jac[1]);
+            const C cz = -(jz0[i] * A.tc.gL[lk] * A.jac[2]) - (jz1[i] * A.tc.gR[lk] * A.jac[2]);
+            rt[i] = rvol + (cx + cy + cz);
+        }
+        S* dst = A.u_out + v * m.npts + ec * NE + 4 * l;
+        if (defer) {
+            stg4<S, C>(dst, rt);
+            continue;
+        }
+        P un[4], u0v[4], out[4];
+        ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, un);
+        if (A.flags & kHasU0) ldc4<S, P>(A.u0 + v * m.npts + ec * NE + 4 * l, u0v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            P o = A.rb * un[i] + A.rc * (P)rt[i];
+            if (A.flags & kHasU0) o = A.ra * u0v[i] + A.rb * un[i] + A.rc * (P)rt[i];
+            out[i] = o;
+        }
+        stg4<S, P>(dst, out);
+    }
+}
+
+// One tile of phase A: EPB elements starting at A.e0 + tile * EPB, LPE
+// threads each. Called by every thread of the block (it synchronises).
 template <class S, class P, class C, class M, int FLUX, int EPB>
-__global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S, P, C> A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void stage_a_tile(const StageAParams<S, P, C>& A, unsigned char* smem_raw,
+                                             long long tile) {
     const int l = threadIdx.x & (LPE - 1);
     const int es = threadIdx.x / LPE;
     const int swz = (es & 1) << 3;
     SlotA<P, C>& sm = reinterpret_cast<SlotA<P, C>*>(smem_raw)[es];
-    const long long e = A.e0 + (long long)blockIdx.x * EPB + es;
+    const long long e = A.e0 + tile * EPB + es;
     const bool live = e < A.e1;
     const long long ec = live ? e : 0;
     const Mesh& m = A.m;
@@ -515,7 +574,7 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
             C praw;
             FaceState<C> s = make_face_state<M, C, P>(qp, praw);
             C F[3][NV];
-            volume_fluxes<C>(s, praw, g, A.mu, F);
+            volume_fluxes<C>(s, praw, g, viscosity<M>(A.mu, A.suth, s), F);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 sm.g[v][p] = F[1][v];
@@ -534,50 +593,13 @@ __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S
     __syncthreads();
 
     // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
-    if (!live) return;
-    const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
-    const int px = sw(4 * l, swz);
-    const bool defer = (A.flags & kDeferRK) != 0;
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        C dx[4], dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
-        ld4s(&sm.g[10 + v][px], dx);
-        ld4s(&divy[v * NE + px], dy);
-        ld4s(&sm.g[5 + v][px], dz);
-        ld4s(&sm.j[2][v][4 * lk], jy0);
-        ld4s(&sm.j[3][v][4 * lk], jy1);
-        ld4s(&sm.j[4][v][4 * lj], jz0);
-        ld4s(&sm.j[5][v][4 * lj], jz1);
-        const C jx0 = sm.j[0][v][l], jx1 = sm.j[1][v][l];
-        C rt[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            C rvol = -((dx[i] + dy[i]) + dz[i]);
-            if (v == 1) rvol += A.forcing;
-            if constexpr (sizeof(C) == 8) {
-                if (A.flags & kRoundRhs) rvol = (C)(float)rvol;
-            }
-            const C cx = -(jx0 * A.tc.gL[i] * A.jac[0]) - (jx1 * A.tc.gR[i] * A.jac[0]);
-            const C cy = -(jy0[i] * A.tc.gL[lj] * A.jac[1]) - (jy1[i] * A.tc.gR[lj] * A.jac[1]);
-            const C cz = -(jz0[i] * A.tc.gL[lk] * A.jac[2]) - (jz1[i] * A.tc.gR[lk] * A.jac[2]);
-            rt[i] = rvol + (cx + cy + cz);
-        }
-        S* dst = A.u_out + v * m.npts + ec * NE + 4 * l;
-        if (defer) {
-            stg4<S, C>(dst, rt);
-            continue;
-        }
-        P un[4], u0v[4], out[4];
-        ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, un);
-        if (A.flags & kHasU0) ldc4<S, P>(A.u0 + v * m.npts + ec * NE + 4 * l, u0v);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            P o = A.rb * un[i] + A.rc * (P)rt[i];
-            if (A.flags & kHasU0) o = A.ra * u0v[i] + A.rb * un[i] + A.rc * (P)rt[i];
-            out[i] = o;
-        }
-        stg4<S, P>(dst, out);
-    }
+    if (live) stage_a_update<S, P, C>(A, sm, ec, l, swz, divy);
+}
+
+template <class S, class P, class C, class M, int FLUX, int EPB>
+__global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S, P, C> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    stage_a_tile<S, P, C, M, FLUX, EPB>(A, smem_raw, blockIdx.x);
 }
 
 template <class S, class P, class C>
@@ -603,10 +625,23 @@ struct StageBParams {
 // added to the new state (times rc), or (deferred RK) folded into
 // u_out = ra*u0 + rb*u_in + rc*(RHS + lift). 16 threads per element, each the
 // x-line l = j + 4k (128-bit accesses).
-template <class S, class P, class C, int EPB>
-__global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
+// Scalar load of data written earlier by the same kernel (COH) or by an
+// earlier launch (read-only path).
+template <bool COH, class T>
+__device__ __forceinline__ T ldf(const T* p) {
+    if constexpr (COH)
+        return *p;
+    else
+        return __ldg(p);
+}
+
+// One tile of phase B: EPB elements starting at B.e0 + tile * EPB. COH: the
+// face buffers and the RHS were written by this same launch (a persistent
+// kernel after its grid barrier), so they are read through the coherent path.
+template <class S, class P, class C, int EPB, bool COH>
+__device__ __forceinline__ void stage_b_tile(const StageBParams<S, P, C>& B, long long tile) {
     const int l = threadIdx.x & (LPE - 1);
-    const long long e = B.e0 + (long long)blockIdx.x * EPB + threadIdx.x / LPE;
+    const long long e = B.e0 + tile * EPB + threadIdx.x / LPE;
     const Mesh& m = B.m;
     if (e >= B.e1) return;
     const int ex = (int)(e % m.nx);
@@ -623,7 +658,7 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
         C acc[4] = {(C)0, (C)0, (C)0, (C)0};
         // interface fluxes of the plus faces: the plus neighbour's minus-face record
         {
-            const C f0 = __ldg(B.fi + ((nxp * 3 + 0) * NV + v) * NF + l);
+            const C f0 = ldf<COH>(B.fi + ((nxp * 3 + 0) * NV + v) * NF + l);
 #pragma unroll
             for (int i = 0; i < 4; ++i) acc[i] = fma(-B.jac[0] * B.tc.gR[i], f0, acc[i]);
         }
@@ -645,8 +680,8 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
             // viscous: the neighbour's record of the shared face is its opposite side
             const int q = v - 1;
             {
-                const C a0 = __ldg(B.fv + ((nxm * 6 + 1) * 4 + q) * NF + l);
-                const C a1 = __ldg(B.fv + ((nxp * 6 + 0) * 4 + q) * NF + l);
+                const C a0 = ldf<COH>(B.fv + ((nxm * 6 + 1) * 4 + q) * NF + l);
+                const C a1 = ldf<COH>(B.fv + ((nxp * 6 + 0) * 4 + q) * NF + l);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, fma(hx * B.tc.gR[i], a1, acc[i]));
             }
@@ -678,7 +713,10 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
         if (defer) {
             C r[4];
             P un[4], u0v[4];
-            ldg4<S, C>(B.rhs + off, r);
+            if constexpr (COH)
+                ldc4<S, C>(B.rhs + off, r);
+            else
+                ldg4<S, C>(B.rhs + off, r);
             ldg4<S, P>(B.u_in + off, un);
             if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, u0v);
 #pragma unroll
@@ -696,6 +734,11 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
         }
         stg4<S, P>(B.u_out + off, out);
     }
+}
+
+template <class S, class P, class C, int EPB>
+__global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
+    stage_b_tile<S, P, C, EPB, false>(B, blockIdx.x);
 }
 
 }  // namespace od

@@ -235,6 +235,18 @@ int main(int argc, char** argv) {
             die("precision_form = \"mixed\" needs u_real = \"f64\" and compute_real = \"f32\"");
     }
     if (const Value* v = R.get("b200", "device")) p.device = (int)R.integer(*v, "device");
+    if (const Value* v = R.get("b200", "viscosity_model")) {
+        if (enum_of(R.str(*v, "viscosity_model"), {"reference", "sutherland"}, "[b200] viscosity_model") == "sutherland") {
+            p.viscosity_model = OD_VISC_SUTHERLAND;
+            p.t_ref = R.get("physics", "t_ref") ? R.f32(R.number(*R.get("physics", "t_ref"), "t_ref")) : (double)273.15f;
+            p.s_suth = R.get("physics", "s_suth") ? R.f32(R.number(*R.get("physics", "s_suth"), "s_suth")) : (double)110.4f;
+        }
+    }
+    if (const Value* v = R.get("b200", "re_bulk")) {
+        const double re = R.number(*v, "re_bulk");
+        if (!(re > 0)) die("[b200] re_bulk must be a positive number");
+        p.mu = R.f32(R.number(R.req("physics", "mach_bulk"), "mach_bulk")) * (0.5 * p.ly) / re;
+    }
 
     const char* tn[2] = {"F32", "F64"};
     std::printf("Configuring pipeline with precisions:\n");

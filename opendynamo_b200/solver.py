@@ -27,8 +27,11 @@ def fr_tables() -> dict:
 
 def make_params(nx, ny, nz, lx, ly, lz, flux="slau2", y_wall=True, u_real="f32", q_real=None,
                 rhs_real=None, compute_real=None, mixed=False, mu=1.6e-4, forcing=1e-3,
-                device=0, fast_math=True, ref_compat=0) -> N.OdParams:
-    """Build od_params. Extents are rounded to f32 as config.rs stores them."""
+                device=0, fast_math=True, ref_compat=0, viscosity_model="fixed", t_ref=273.15,
+                s_suth=110.4) -> N.OdParams:
+    """Build od_params. Extents are rounded to f32 as config.rs stores them.
+    viscosity_model "sutherland" is an extension (the reference keeps mu
+    constant whatever its config says)."""
     q_real = q_real or (u_real if not mixed else "f32")
     rhs_real = rhs_real or (u_real if not mixed else "f32")
     compute_real = compute_real or (u_real if not mixed else "f32")
@@ -36,15 +39,20 @@ def make_params(nx, ny, nz, lx, ly, lz, flux="slau2", y_wall=True, u_real="f32",
     return N.OdParams(int(nx), int(ny), int(nz), float(np.float32(lx)), float(np.float32(ly)),
                       float(np.float32(lz)), N.OD_FLUX[flux], int(bool(y_wall)), t[u_real], t[q_real],
                       t[rhs_real], t[compute_real], int(bool(mixed)), int(bool(fast_math)), float(mu),
-                      float(forcing), int(device), int(ref_compat))
+                      float(forcing), int(device), int(ref_compat),
+                      {"fixed": N.OD_VISC_CONSTANT, "sutherland": N.OD_VISC_SUTHERLAND}[viscosity_model],
+                      float(t_ref), float(s_suth))
 
 
 def params_from_config(cfg: Config, device: int = 0) -> N.OdParams:
     m, pr = cfg.mesh, cfg.precision
     return make_params(m.nx, m.ny, m.nz, m.lx, m.ly, m.lz, cfg.solver.flux_scheme,
                        cfg.physics.y_boundary == "wall", pr.u_real, pr.q_real, pr.rhs_real,
-                       pr.compute_real, cfg.b200.precision_form == "mixed", cfg.b200.mu,
-                       cfg.b200.forcing, device, cfg.solver.fast_math)
+                       pr.compute_real, cfg.b200.precision_form == "mixed",
+                       cfg.b200.effective_mu(cfg.physics.mach_bulk, m.ly), cfg.b200.forcing, device,
+                       cfg.solver.fast_math, 0,
+                       "sutherland" if cfg.b200.viscosity_model == "sutherland" else "fixed",
+                       cfg.physics.t_ref, cfg.physics.s_suth)
 
 
 class Solver:
@@ -104,6 +112,21 @@ class Solver:
             out = np.empty(5 * self.npts, dtype=self.dtype)
         self._chk(self._lib.od_get_state(self._ctx, out.ctypes.data_as(ctypes.c_void_p), out.nbytes),
                   "od_get_state")
+        return out
+
+    def diagnostics(self, profiles: bool = True) -> dict:
+        """Volume integrals and x-z plane-averaged profiles of the current
+        state (od_diagnostics). Profiles: (ny*4, 8) rows bottom to top of
+        <rho> <u> <v> <w> <uu> <vv> <ww> <uv>."""
+        vol = np.zeros(6)
+        prof = np.zeros(self.params.ny * 4 * 8) if profiles else None
+        self._chk(self._lib.od_diagnostics(self._ctx, vol.ctypes.data_as(ctypes.c_void_p),
+                                           prof.ctypes.data_as(ctypes.c_void_p) if profiles else None,
+                                           0 if prof is None else prof.size), "od_diagnostics")
+        out = {"mass": vol[0], "momentum_x": vol[1], "energy": vol[2], "kinetic_energy": vol[3],
+               "enstrophy": vol[4], "volume": vol[5]}
+        if profiles:
+            out["profiles"] = prof.reshape(-1, 8)
         return out
 
     def set_state_device(self, ptr: int, nbytes: int) -> None:

@@ -27,6 +27,7 @@ class OrcParams(ctypes.Structure):
         ("rhs_f64", ctypes.c_int), ("c_f64", ctypes.c_int),
         ("mu", ctypes.c_double), ("forcing", ctypes.c_double),
         ("threads", ctypes.c_int), ("ref_y_slice_f32", ctypes.c_int),
+        ("suth", ctypes.c_double),
     ]
 
 
@@ -44,6 +45,7 @@ def lib():
         L.orc_fr_tables.argtypes = [vp]
         L.orc_euler_flux.argtypes = [ctypes.c_int, vp, vp]
         L.orc_viscous_flux.argtypes = [ctypes.c_int, ctypes.c_double, vp, vp, vp]
+        L.orc_viscous_flux_suth.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp, vp]
         L.orc_riemann_flux.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.orc_volume.argtypes = [P, vp, vp, ctypes.POINTER(vp)]
         L.orc_faces.argtypes = [P, vp, ctypes.POINTER(vp), ctypes.POINTER(vp)]
@@ -62,14 +64,17 @@ def _ptr(a: np.ndarray):
 
 
 def make_params(nx, ny, nz, lx, ly, lz, flux="rusanov", y_wall=False, u="f64", q=None, rhs=None,
-                compute=None, mu=1.6e-4, forcing=1e-3, threads=0, ref_y_slice_f32=False) -> OrcParams:
+                compute=None, mu=1.6e-4, forcing=1e-3, threads=0, ref_y_slice_f32=False,
+                sutherland=None) -> OrcParams:
+    """sutherland: None (constant mu, the reference) or (t_ref, s_suth)."""
     q = q or u
     rhs = rhs or u
     compute = compute or u
     return OrcParams(nx, ny, nz, float(np.float32(lx)), float(np.float32(ly)), float(np.float32(lz)),
                      FLUX_IDS[flux], int(bool(y_wall)), int(u == "f64"), int(q == "f64"),
                      int(rhs == "f64"), int(compute == "f64"), float(mu), float(forcing), int(threads),
-                     int(bool(ref_y_slice_f32)))
+                     int(bool(ref_y_slice_f32)),
+                     -1.0 if sutherland is None else float(sutherland[1]) / float(sutherland[0]))
 
 
 def _dt(flag):
@@ -91,11 +96,14 @@ def euler_flux(d, q):
     return f
 
 
-def viscous_flux(d, q, g, mu=1.6e-4):
+def viscous_flux(d, q, g, mu=1.6e-4, sutherland=None):
     q = np.ascontiguousarray(q, dtype=np.float64)
     g = np.ascontiguousarray(g, dtype=np.float64)
     f = np.zeros(5)
-    lib().orc_viscous_flux(d, mu, _ptr(q), _ptr(g), _ptr(f))
+    if sutherland is None:
+        lib().orc_viscous_flux(d, mu, _ptr(q), _ptr(g), _ptr(f))
+    else:
+        lib().orc_viscous_flux_suth(d, mu, float(sutherland[1]) / float(sutherland[0]), _ptr(q), _ptr(g), _ptr(f))
     return f
 
 

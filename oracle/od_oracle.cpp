@@ -118,6 +118,14 @@ Tables fr_tables() {
 template <class C>
 struct Phys {
     C mu;
+    C suth = (C)-1.0;  // Sutherland S = s_suth / t_ref; < 0: constant mu
+
+    // mu * T^1.5 (1 + S) / (T + S), T = gamma * p / rho with the clamped pressure
+    C mu_at(const C* q) const {
+        if (suth < (C)0.0) return mu;
+        C T = gam * pressure(q) / q[0];
+        return mu * T * std::sqrt(T) * ((C)1.0 + suth) / (T + suth);
+    }
     const C gam = (C)1.4;
     const C pr = (C)0.72;
 
@@ -140,6 +148,7 @@ struct Phys {
 
     // g[3*var + dir]; the stress/heat-flux algebra of device_functions.cuh:23-102.
     void viscous(int d, const C* q, const C* g, C* f) const {
+        const C mu = mu_at(q);
         C r = q[0];
         C vel[3] = {q[1] / r, q[2] / r, q[3] / r};
         // dvel[a][b] = d(vel_a)/d(x_b)
@@ -304,6 +313,7 @@ typedef struct {
     double forcing; // reference: 1e-3 on rho*u (rhs.cu:508)
     int threads;    // 0 = all host threads
     int ref_y_slice_f32;  // f64 compute: y slices with f32 products and pair sums, as rhs.cu:145-160
+    double suth;          // Sutherland S = s_suth / t_ref (extension); < 0: constant mu as the reference
 } orc_params;
 
 }  // extern "C"
@@ -330,6 +340,7 @@ struct Oracle {
         }
         for (int i = 0; i < NP * NP; ++i) D[i] = (C)T.D[i];
         ph.mu = (C)p.mu;
+        ph.suth = (C)p.suth;
         nelem = (long)p.nx * p.ny * p.nz;
         npts = nelem * NE;
         C L[3] = {(C)p.lx, (C)p.ly, (C)p.lz};
@@ -741,6 +752,14 @@ int orc_euler_flux(int d, const double* q, double* f) {
 int orc_viscous_flux(int d, double mu, const double* q, const double* g, double* f) {
     Phys<double> ph;
     ph.mu = mu;
+    ph.viscous(d, q, g, f);
+    return 0;
+}
+// Same with Sutherland's law (suth = s_suth / t_ref; < 0: constant mu).
+int orc_viscous_flux_suth(int d, double mu, double suth, const double* q, const double* g, double* f) {
+    Phys<double> ph;
+    ph.mu = mu;
+    ph.suth = suth;
     ph.viscous(d, q, g, f);
     return 0;
 }

@@ -102,3 +102,26 @@ def test_mixed_precision_form_requires_f64_state():
         parse_config(data)
     data["precision"]["u_real"] = "f64"
     assert parse_config(data).b200.precision_form == "mixed"
+
+
+def test_b200_viscosity_extensions():
+    import tomllib
+    from opendynamo_b200 import _native as N
+    from opendynamo_b200.solver import params_from_config
+    data = tomllib.loads(MINIMAL)
+    # the reference's own viscosity keys change nothing
+    data["physics"]["viscosity_model"] = "sutherland"
+    p = params_from_config(parse_config(data))
+    assert p.viscosity_model == N.OD_VISC_CONSTANT and p.mu == 1.6e-4
+    data["b200"] = {"viscosity_model": "sutherland", "re_bulk": 3000}
+    data["physics"]["t_ref"] = 300.0
+    cfg = parse_config(data)
+    p = params_from_config(cfg)
+    assert p.viscosity_model == N.OD_VISC_SUTHERLAND and (p.t_ref, p.s_suth) == (300.0, float(np.float32(110.4)))
+    assert p.mu == float(np.float32(0.2)) * 1.0 / 3000
+    data["b200"] = {"viscosity_model": "power"}
+    with pytest.raises(ConfigError, match="viscosity_model"):
+        parse_config(data)
+    data["b200"] = {"re_bulk": -1}
+    with pytest.raises(ConfigError, match="re_bulk"):
+        parse_config(data)

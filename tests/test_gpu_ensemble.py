@@ -1,0 +1,112 @@
+"""The batching form on the GPU: boxes of uneven size with mixed schemes,
+walls, viscosities and time steps advanced by one persistent launch per RK
+stage agree box by box with advancing each box alone (to f32 round-off: the
+ensemble kernel contracts a few multiply-adds differently); the grid size and
+the CUDA graph change no bit; the autotuner reports its trials and restores
+the states."""
+
+import math
+
+import numpy as np
+import pytest
+
+from helpers import random_smooth, rel_l2
+from opendynamo_b200.forms.ensemble import Box, Ensemble, benchmark_boxes
+from opendynamo_b200.solver import Solver
+
+BOXES = [
+    Box((3, 2, 4), (2 * math.pi, 2.0, math.pi), "slau2", True, 1.6e-4, 1e-3, 1e-3),
+    Box((2, 2, 2), (2 * math.pi,) * 3, "rusanov", False, 5e-4, 0.0, 2e-3),
+    Box((4, 3, 2), (1.0, 2.0, 3.0), "ausm+", True, 1e-3, 1e-3, 5e-4),
+    Box((5, 1, 3), (2 * math.pi, 2.0, math.pi), "rusanov", True, 0.0, 0.0, 1e-3),
+    Box((1, 4, 1), (1.0, 1.0, 1.0), "slau2", False, 2e-4, 1e-3, 7e-4),
+]
+
+
+def _states(boxes):
+    return [random_smooth(*b.n, seed=10 + k, dtype=np.float32) for k, b in enumerate(boxes)]
+
+
+def _close(got, want):
+    """f32 round-off: the two kernels differ in a few last bits."""
+    assert np.all(rel_l2(got, want) < 1e-7), rel_l2(got, want)
+    assert np.abs(got.astype(np.float64) - want).max() < 1e-6
+
+
+def _alone(boxes, states, steps):
+    out = []
+    for b, u in zip(boxes, states):
+        with Solver(b.params()) as s:
+            s.set_state(u)
+            s.step(steps, float(np.float32(b.dt)))
+            out.append(s.get_state())
+    return out
+
+
+@pytest.mark.gpu
+def test_ensemble_equals_boxes_alone():
+    states = _states(BOXES)
+    want = _alone(BOXES, states, 4)
+    with Ensemble(BOXES) as E:
+        info = E.info()
+        assert info["grid"] > 0
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.step(4)
+        first = [E.get_state(k) for k in range(len(BOXES))]
+        for k in range(len(BOXES)):
+            _close(first[k], want[k])
+        # deterministic: the same steps again give the same bytes
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.step(4)
+        for k in range(len(BOXES)):
+            assert E.get_state(k).tobytes() == first[k].tobytes(), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("epb", [2, 4])
+def test_ensemble_shape_does_not_change_results(epb):
+    states = _states(BOXES)
+    want = _alone(BOXES, states, 3)
+    runs = []
+    for bps, graph in [(0, True), (1, True), (1, False), (2, False)]:
+        with Ensemble(BOXES) as E:
+            E.set_shape(epb, bps, graph)
+            for k, u in enumerate(states):
+                E.set_state(k, u)
+            E.step(3)
+            runs.append([E.get_state(k) for k in range(len(BOXES))])
+    for k in range(len(BOXES)):
+        _close(runs[0][k], want[k])
+        for r in runs[1:]:
+            assert r[k].tobytes() == runs[0][k].tobytes(), k
+
+
+@pytest.mark.gpu
+def test_autotune_and_benchmark_boxes():
+    boxes = benchmark_boxes(count=6, n_min=2, n_max=5)
+    assert len({b.flux for b in boxes}) >= 1 and all(2 <= b.n[0] <= 5 for b in boxes)
+    states = [b.initial_state() for b in boxes]
+    want = _alone(boxes, states, 2)
+    with Ensemble(boxes) as E:
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        rep = E.autotune(trial_steps=1)
+        assert "chosen:" in rep and "ms/step" in rep
+        # the autotuner restores the states it stepped
+        for k, u in enumerate(states):
+            assert E.get_state(k).tobytes() == u.tobytes()
+        E.step(2)
+        for k in range(len(boxes)):
+            _close(E.get_state(k), want[k])
+
+
+def test_benchmark_boxes_are_seeded():
+    a, b = benchmark_boxes(), benchmark_boxes()
+    assert len(a) == 64 and [x.n for x in a] == [x.n for x in b]
+    ns = np.array([x.n[0] for x in a])
+    assert ns.min() >= 8 and ns.max() <= 32
+    mach = np.array([x.mach for x in a])
+    assert mach.min() >= 0.05 and mach.max() <= 0.3
+    assert {x.flux for x in a} == {"rusanov", "slau2"} and {x.kind for x in a} == {"tgv", "channel"}

@@ -206,3 +206,25 @@ def test_oracle_matches_reference_tgv_20_steps():
     p = oracle.make_params(n, n, n, L, L, L, flux="rusanov", y_wall=False, u="f64", ref_y_slice_f32=True)
     out = oracle.run(p, d["u"], int(d["steps"]), float(d["dt"]))
     assert np.all(rel_l2(out, d["out"]) < 1e-12)
+
+
+def test_sutherland_law_pointwise():
+    """Viscous flux with Sutherland's law = constant-mu flux with
+    mu * T^1.5 (1 + S) / (T + S), T = gamma p / rho (1 at rho = 1, p = 1/gamma)."""
+    rng = np.random.default_rng(4)
+    S = 110.4 / 273.15
+    for d in range(3):
+        for _ in range(5):
+            rho = 0.8 + 0.4 * rng.random()
+            vel = 0.3 * rng.standard_normal(3)
+            p = 0.5 + 0.5 * rng.random()
+            q = np.array([rho, *(rho * vel), p / 0.4 + 0.5 * rho * vel @ vel])
+            g = rng.standard_normal(15)
+            T = 1.4 * p / rho
+            want = oracle.viscous_flux(d, q, g, mu=2e-3 * T ** 1.5 * (1 + S) / (T + S))
+            got = oracle.viscous_flux(d, q, g, mu=2e-3, sutherland=(273.15, 110.4))
+            np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-18)
+    q = np.array([1.0, 0.1, 0.0, 0.0, (1 / 1.4) / 0.4 + 0.005])
+    g = rng.standard_normal(15)
+    np.testing.assert_allclose(oracle.viscous_flux(0, q, g, mu=2e-3, sutherland=(273.15, 110.4)),
+                               oracle.viscous_flux(0, q, g, mu=2e-3), rtol=1e-14, atol=1e-18)
