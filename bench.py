@@ -352,7 +352,9 @@ def run_closure_form(args, world, rank, local):
     log = lambda m: print(m, file=sys.stderr, flush=True)
     data = CL.generate_data(cfg, device=local, log=log)
     net, tr = CL.train(data, cfg, device=local, log=log)
-    norm = {"mean": data["mean"].tolist(), "scale": data["scale"].tolist(), "out_scale": data["out_scale"].tolist()}
+    alpha, cal = CL.calibrate(net, data, cfg, device=local, log=log)
+    norm = {"mean": data["mean"].tolist(), "scale": data["scale"].tolist(), "out_scale": data["out_scale"].tolist(),
+            "alpha": alpha, "calibration": [(a, e) for a, e in cal]}
     del data
     torch.cuda.empty_cache()
     ev = CL.evaluate(net, cfg, device=local, log=log)
@@ -360,7 +362,7 @@ def run_closure_form(args, world, rank, local):
         p = net.get_params()
         np.savez_compressed(args.save_weights, **p, mean=np.array(norm["mean"], np.float32),
                             scale=np.array(norm["scale"], np.float32),
-                            out_scale=np.array(norm["out_scale"], np.float32))
+                            out_scale=np.array(norm["out_scale"], np.float32), alpha=np.float32(alpha))
     net.close()
     w = ev["wall_ms"]
     speed = w["plain_mid"] / max(w["closure_coarse"], 1e-9)

@@ -308,7 +308,7 @@ void* od_ensemble_stream(od_ensemble* e);
 
 /* BF16 tensor-core GEMM of the closure network (tcgen05, fp32 accumulation
  * in tensor memory): C[M x N] (+ bias[N]) = A[M x K] * B[N x K]^T, A and B
- * bf16 row-major in device memory, C fp32. M % 128 == 0, N % 128 == 0,
+ * bf16 row-major in device memory, C fp32. M % 128 == 0, N % 64 == 0,
  * K % 64 == 0. Synchronous on `stream`. Exposed for tests; the closure uses
  * the same kernel with fused epilogues. No reference counterpart. */
 int od_gemm_bf16(int M, int N, int K, const void* dA, const void* dB, float* dC, const float* dbias, void* stream);

@@ -8,7 +8,8 @@
 //             fine elements, the coarse mass matrix is diagonal at the GL
 //             points)
 //   features  64 points x (5 conserved + 9 velocity gradients) per element,
-//             standardised with per-channel constants, bf16 rows
+//             standardised with per-channel constants and clipped to +-8,
+//             bf16 rows
 //   apply     rhs += out_scale[v] * network output (between the two phases
 //             of an RK stage)
 //   training  loss gradient, bias gradients, gathers and Adam
@@ -29,7 +30,7 @@
 namespace od {
 TablesD host_fr_tables();
 namespace mlp {
-cudaError_t launch_gemm(const GemmArgs& g, int epi, cudaStream_t s);
+cudaError_t launch_gemm(const GemmArgs& g, int epi, cudaStream_t s, size_t ws_floats);
 }
 }  // namespace od
 
@@ -37,6 +38,7 @@ namespace {
 
 using bf16 = __nv_bfloat16;
 constexpr int kIn = 896, kHid = 256, kOut = 320, kOutPad = 384, kChan = 14;
+constexpr float kClip = 8.0f;  // standardised inputs are clipped to +-kClip (states outside the training range)
 
 // ---------------------------------------------------------------- projection
 struct ProjParams {
@@ -163,7 +165,8 @@ __global__ void __launch_bounds__(64) features_kernel(const T* __restrict__ u, F
     bf16* row = X + e * kIn;
 #pragma unroll
     for (int ch_i = 0; ch_i < kChan; ++ch_i)
-        row[ch_i * 64 + p] = __float2bfloat16_rn((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i]);
+        row[ch_i * 64 + p] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i],
+                                                             -kClip), kClip));
 }
 
 FeatParams feat_params(int nx, int ny, int nz, double lx, double ly, double lz, const float* mean,
@@ -223,13 +226,22 @@ __global__ void loss_grad_kernel(const float* __restrict__ Y, const float* __res
     if ((threadIdx.x & 31) == 0 && sq != 0.f) atomicAdd(loss, (double)sq);
 }
 
-// out[n] = sum_m A[m][n] (bf16 -> fp32)
-__global__ void colsum_kernel(const bf16* __restrict__ A, int M, int N, float* __restrict__ out) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
+// out[n] = sum_m AT[n][m] (bf16 -> fp32): bias gradients from the transposed
+// copies, one block per row, coalesced
+__global__ void __launch_bounds__(256) rowsum_kernel(const bf16* __restrict__ AT, int M, float* __restrict__ out) {
+    __shared__ float red[8];
+    const bf16* row = AT + (long long)blockIdx.x * M;
     float s = 0.f;
-    for (int m = 0; m < M; ++m) s += __bfloat162float(A[(long long)m * N + n]);
-    out[n] = s;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) s += __bfloat162float(row[m]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        out[blockIdx.x] = t;
+    }
 }
 
 // rows of a bf16 pool (and a bf16 target pool) into a batch: X [M x 896], X^T, T [M x 384] fp32
@@ -311,6 +323,8 @@ struct od_mlp {
     long long* rows_d = nullptr;
     double* loss = nullptr;
     int* err = nullptr;
+    float* ws = nullptr;            // split-K partial sums of the weight gradients
+    size_t ws_floats = 0;
     long long step = 0;
     std::string msg;
     // closure attachment (features of the coarse state + output scaling)
@@ -343,22 +357,30 @@ cudaError_t gemm(od_mlp* m, const bf16* A, const bf16* B, int M, int N, int K, i
     a.out_bfT = obfT;
     a.z_in = zin;
     a.err = m->err;
-    return od::mlp::launch_gemm(a, epi, m->stream);
+    a.ws = m->ws;
+    return od::mlp::launch_gemm(a, epi, m->stream, m->ws_floats);
 }
 
-// forward of M rows of X (bf16 [M x 896]); training keeps transposed activations
-cudaError_t forward(od_mlp* m, const bf16* X, int M, float* Y, bool keep_t) {
+// hidden layers of M rows of X (bf16 [M x 896]); training keeps the
+// pre-activations and the transposed activations
+cudaError_t hidden(od_mlp* m, const bf16* X, int M, bool train) {
     cudaError_t e = cudaSuccess;
     const bf16* in = X;
     int kin = kIn;
     for (int l = 0; l < 3 && e == cudaSuccess; ++l) {
-        e = gemm(m, in, m->wb[l], M, kHid, kin, od::mlp::kBiasGelu, m->w + m->off_b[l], m->Z[l], m->A[l],
-                 keep_t ? m->AT[l] : nullptr, nullptr);
+        e = gemm(m, in, m->wb[l], M, kHid, kin, od::mlp::kBiasGelu, m->w + m->off_b[l], train ? m->Z[l] : nullptr,
+                 m->A[l], train ? m->AT[l] : nullptr, nullptr);
         in = m->A[l];
         kin = kHid;
     }
+    return e;
+}
+
+// forward of M rows of X into Y [M x 384]
+cudaError_t forward(od_mlp* m, const bf16* X, int M, float* Y, bool keep_t) {
+    cudaError_t e = hidden(m, X, M, keep_t);
     if (e == cudaSuccess)
-        e = gemm(m, in, m->wb[3], M, kOutPad, kHid, od::mlp::kStoreF32, m->w + m->off_b[3], Y, nullptr, nullptr,
+        e = gemm(m, m->A[2], m->wb[3], M, kOutPad, kHid, od::mlp::kStoreF32, m->w + m->off_b[3], Y, nullptr, nullptr,
                  nullptr);
     return e;
 }
@@ -374,7 +396,7 @@ cudaError_t backward(od_mlp* m, const bf16* XT, int M, int mv) {
     if (e == cudaSuccess)
         e = gemm(m, m->dYT, m->AT[2], kOutPad, kHid, M, od::mlp::kStoreF32, nullptr, m->g + m->off_w[3], nullptr,
                  nullptr, nullptr);
-    colsum_kernel<<<blocks(kOutPad, 128), 128, 0, m->stream>>>(m->dY, M, kOutPad, m->g + m->off_b[3]);
+    rowsum_kernel<<<kOutPad, 256, 0, m->stream>>>(m->dYT, M, m->g + m->off_b[3]);
     if (e == cudaSuccess)
         e = gemm(m, m->dY, m->wbT[3], M, kHid, kOutPad, od::mlp::kGeluGrad, nullptr, nullptr, m->dZa, m->dZaT,
                  m->Z[2]);
@@ -385,7 +407,7 @@ cudaError_t backward(od_mlp* m, const bf16* XT, int M, int mv) {
         const int kin = l == 0 ? kIn : kHid;
         e = gemm(m, dzT, inT, kHid, kin, M, od::mlp::kStoreF32, nullptr, m->g + m->off_w[l], nullptr, nullptr,
                  nullptr);
-        colsum_kernel<<<blocks(kHid, 128), 128, 0, m->stream>>>(dz, M, kHid, m->g + m->off_b[l]);
+        rowsum_kernel<<<kHid, 256, 0, m->stream>>>(dzT, M, m->g + m->off_b[l]);
         if (e == cudaSuccess && l > 0) {
             e = gemm(m, dz, m->wbT[l], M, kHid, kHid, od::mlp::kGeluGrad, nullptr, nullptr, nz, nzT, m->Z[l - 1]);
             std::swap(dz, nz);
@@ -466,6 +488,8 @@ int od_mlp_create(int max_rows, int device, od_mlp** out) {
     mal((void**)&m->rows_d, sizeof(long long) * M);
     mal((void**)&m->loss, sizeof(double));
     mal((void**)&m->err, sizeof(int));
+    m->ws_floats = (size_t)32 * kOutPad * kIn;
+    mal((void**)&m->ws, sizeof(float) * m->ws_floats);
     if (e != cudaSuccess) return mfail(m, OD_ERR_CUDA, std::string("od_mlp_create: ") + cudaGetErrorString(e));
     return OD_OK;
 }
@@ -477,7 +501,7 @@ void od_mlp_destroy(od_mlp* m) {
     void* ps[] = {m->w, m->m1, m->m2, m->g, m->wb[0], m->wb[1], m->wb[2], m->wb[3], m->wbT[0], m->wbT[1], m->wbT[2],
                   m->wbT[3], m->Z[0], m->Z[1], m->Z[2], m->A[0], m->A[1], m->A[2], m->AT[0], m->AT[1], m->AT[2],
                   m->Y, m->dY, m->dYT, m->dZa, m->dZaT, m->dZb, m->dZbT, m->X, m->XT, m->T, m->rows_d, m->loss,
-                  m->err, m->Xc, m->Yc};
+                  m->err, m->Xc, m->Yc, m->ws};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -660,22 +684,38 @@ cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStre
     else
         features_kernel<float><<<(unsigned)m->nelem_c, 64, 0, s>>>((const float*)u_in, m->fp, m->Xc);
     e = cudaGetLastError();
-    // the network runs on the solver's stream
+    // the network runs on the solver's stream; the last layer's epilogue adds
+    // out_scale * (output) into the RHS directly (f32 state)
     cudaStream_t keep = m->stream;
     m->stream = s;
-    if (e == cudaSuccess) e = forward(m, m->Xc, (int)m->mpad_c, m->Yc, false);
-    m->stream = keep;
-    const long long n = m->nelem_c * 64 * 5;
+    if (e == cudaSuccess) e = hidden(m, m->Xc, (int)m->mpad_c, false);
     if (e == cudaSuccess) {
-        const float* o = m->out_scale;
-        if (m->attached_f64)
-            apply_kernel<double><<<blocks(n, 256), 256, 0, s>>>((double*)rhs, m->Yc, m->nelem_c, o[0], o[1], o[2], o[3],
-                                                                o[4]);
-        else
-            apply_kernel<float><<<blocks(n, 256), 256, 0, s>>>((float*)rhs, m->Yc, m->nelem_c, o[0], o[1], o[2], o[3],
-                                                               o[4]);
-        e = cudaGetLastError();
+        if (m->attached_f64) {
+            e = gemm(m, m->A[2], m->wb[3], (int)m->mpad_c, kOutPad, kHid, od::mlp::kStoreF32, m->w + m->off_b[3],
+                     m->Yc, nullptr, nullptr, nullptr);
+            const long long n = m->nelem_c * 64 * 5;
+            const float* o = m->out_scale;
+            if (e == cudaSuccess)
+                apply_kernel<double><<<blocks(n, 256), 256, 0, s>>>((double*)rhs, m->Yc, m->nelem_c, o[0], o[1], o[2],
+                                                                    o[3], o[4]);
+        } else {
+            od::mlp::GemmArgs a{};
+            a.A = m->A[2];
+            a.B = m->wb[3];
+            a.M = (int)m->mpad_c;
+            a.N = kOutPad;
+            a.K = kHid;
+            a.bias = m->w + m->off_b[3];
+            a.err = m->err;
+            a.rhs = (float*)rhs;
+            a.rhs_npts = m->nelem_c * 64;
+            a.rhs_rows = (int)m->nelem_c;
+            for (int v = 0; v < 5; ++v) a.rhs_scale[v] = m->out_scale[v];
+            e = od::mlp::launch_gemm(a, od::mlp::kApplyRhs, s, 0);
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
     }
+    m->stream = keep;
     return e;
 }
 

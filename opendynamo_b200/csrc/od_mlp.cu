@@ -11,24 +11,84 @@
 namespace od {
 namespace mlp {
 
+constexpr long long kSMs = 148;  // B200
+
+// out = sum of the ksplit partial tiles (+ bias)
+__global__ void splitk_reduce_kernel(const float* __restrict__ ws, int ks, long long mn, int N,
+                                     const float* __restrict__ bias, float* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mn) return;
+    float v = 0.f;
+    for (int z = 0; z < ks; ++z) v += ws[z * mn + i];
+    if (bias) v += bias[i % N];
+    out[i] = v;
+}
+
 template <int NT, int EPI>
 cudaError_t launch_gemm_t(const GemmArgs& g, cudaStream_t s) {
     const size_t smem = gemm_smem_bytes<NT>();
-    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the shared-memory limit is set once per device (a host call per launch
+    // cost more than the small GEMMs themselves)
+    static bool prepared[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)(g.M / BM), (unsigned)(g.N / NT));
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!prepared[dev]) {
+        e = cudaFuncSetAttribute(gemm_kernel<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        prepared[dev] = true;
+    }
+    const int ks = g.ksplit > 1 ? g.ksplit : 1;
+    dim3 grid((unsigned)(g.M / BM), (unsigned)(g.N / NT), (unsigned)ks);
     gemm_kernel<NT, EPI><<<grid, 128, smem, s>>>(g);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e == cudaSuccess && ks > 1) {
+        const long long mn = (long long)g.M * g.N;
+        splitk_reduce_kernel<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(g.ws, ks, mn, g.N, g.bias, g.out_f32);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
-// C = A B^T with the epilogue `epi`; M % 128 == 0, N % 128 == 0, K % 64 == 0.
-cudaError_t launch_gemm(const GemmArgs& g, int epi, cudaStream_t s) {
-    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.M % BM || g.N % 128 || g.K % BK) return cudaErrorInvalidValue;
-    const bool wide = g.N % 256 == 0;
+template <int EPI>
+cudaError_t launch_nt(const GemmArgs& g, int nt, cudaStream_t s) {
+    if (nt == 256) return launch_gemm_t<256, EPI>(g, s);
+    if (nt == 128) return launch_gemm_t<128, EPI>(g, s);
+    return launch_gemm_t<64, EPI>(g, s);
+}
+
+// C = A B^T with the epilogue `epi`; M % 128 == 0, N % 64 == 0, K % 64 == 0.
+// Tile width: the widest of 256 / 128 / 64 dividing N that still gives two
+// CTAs per SM (the epilogue has four warps per CTA and wants company),
+// else 64. kStoreF32 products with few tiles and a long K (weight gradients)
+// split K when the caller passes a workspace of ksplit * M * N floats.
+cudaError_t launch_gemm(const GemmArgs& g0, int epi, cudaStream_t s, size_t ws_floats) {
+    if (g0.M <= 0 || g0.N <= 0 || g0.K <= 0 || g0.M % BM || g0.N % 64 || g0.K % BK) return cudaErrorInvalidValue;
+    GemmArgs g = g0;
+    const long long rows = g.M / BM;
+    int nt = 64;
+    for (int c : {256, 128}) {
+        if (g.N % c == 0 && rows * (g.N / c) >= 2 * kSMs) {
+            nt = c;
+            break;
+        }
+    }
+    g.ksplit = 1;
+    if (epi == kStoreF32 && g.ws) {
+        const long long tiles = rows * (g.N / nt);
+        const int kblocks = g.K / BK;
+        int ks = 1;
+        while (tiles * ks < 2 * kSMs && kblocks % (2 * ks) == 0 && kblocks / (2 * ks) >= 2 &&
+               (size_t)(2 * ks) * g.M * g.N <= ws_floats)
+            ks *= 2;
+        g.ksplit = ks;
+    }
     switch (epi) {
-        case kStoreF32: return wide ? launch_gemm_t<256, kStoreF32>(g, s) : launch_gemm_t<128, kStoreF32>(g, s);
-        case kBiasGelu: return wide ? launch_gemm_t<256, kBiasGelu>(g, s) : launch_gemm_t<128, kBiasGelu>(g, s);
-        case kGeluGrad: return wide ? launch_gemm_t<256, kGeluGrad>(g, s) : launch_gemm_t<128, kGeluGrad>(g, s);
+        case kStoreF32: return launch_nt<kStoreF32>(g, nt, s);
+        case kBiasGelu: return launch_nt<kBiasGelu>(g, nt, s);
+        case kGeluGrad: return launch_nt<kGeluGrad>(g, nt, s);
+        case kApplyRhs: return launch_nt<kApplyRhs>(g, nt, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -39,11 +99,14 @@ cudaError_t launch_gemm(const GemmArgs& g, int epi, cudaStream_t s) {
 extern "C" int od_gemm_bf16(int M, int N, int K, const void* dA, const void* dB, float* dC, const float* dbias,
                             void* stream) {
     if (!dA || !dB || !dC) return OD_ERR_ARG;
-    if (M <= 0 || N <= 0 || K <= 0 || M % 128 || N % 128 || K % 64) return OD_ERR_ARG;
+    if (M <= 0 || N <= 0 || K <= 0 || M % 128 || N % 64 || K % 64) return OD_ERR_ARG;
     int* err = nullptr;
+    float* ws = nullptr;
     cudaStream_t s = (cudaStream_t)stream;
+    const size_t ws_floats = (size_t)16 * M * N;
     cudaError_t e = cudaMallocAsync((void**)&err, sizeof(int), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&ws, ws_floats * sizeof(float), s);
     od::mlp::GemmArgs g{};
     g.A = (const __nv_bfloat16*)dA;
     g.B = (const __nv_bfloat16*)dB;
@@ -53,10 +116,12 @@ extern "C" int od_gemm_bf16(int M, int N, int K, const void* dA, const void* dB,
     g.bias = dbias;
     g.out_f32 = dC;
     g.err = err;
-    if (e == cudaSuccess) e = od::mlp::launch_gemm(g, od::mlp::kStoreF32, s);
+    g.ws = ws;
+    if (e == cudaSuccess) e = od::mlp::launch_gemm(g, od::mlp::kStoreF32, s, ws_floats);
     int herr = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (err) cudaFreeAsync(err, s);
+    if (ws) cudaFreeAsync(ws, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return OD_ERR_CUDA;
     return herr ? OD_ERR_CUDA : OD_OK;

@@ -3,7 +3,9 @@
 //   C[M x N] = A[M x K] * B[N x K]^T     A, B: bf16, row-major, K contiguous
 //                                        accumulation: fp32 in tensor memory
 //
-// One CTA computes a 128 x NT tile (NT = 128 or 256) with 128 threads:
+// One CTA computes a 128 x NT tile (NT = 64, 128 or 256) with 128 threads,
+// over all of K or over one of `ksplit` K ranges (blockIdx.z; fp32 partial
+// tiles, summed by a second kernel):
 //   - all threads stage 128 x 64 (A) and NT x 64 (B) bf16 blocks into shared
 //     memory with 16-byte cp.async copies, two stages deep, in the canonical
 //     no-swizzle K-major layout of the tensor cores: 8 x 16-byte core
@@ -35,6 +37,7 @@ enum Epi : int {
     kStoreF32 = 0,     // C (+ bias) -> fp32 [M x N] (ldc = N)
     kBiasGelu = 1,     // z = C + bias -> z fp32, gelu(z) -> bf16 [M x N] and bf16 transpose [N x M]
     kGeluGrad = 2,     // dz = C * gelu'(z_in) -> bf16 [M x N] and bf16 transpose [N x M]
+    kApplyRhs = 3,     // rhs[v][row*64 + p] += rhs_scale[v] * (C + bias) for column v*64 + p < 320, row < rows
 };
 
 struct GemmArgs {
@@ -47,6 +50,12 @@ struct GemmArgs {
     __nv_bfloat16* out_bfT;   // transposed copy ([N x M]) or null
     const float* z_in;        // kGeluGrad: the layer's pre-activation [M x N]
     int* err;                 // set to 1 when a bounded wait gives up
+    int ksplit;               // > 1 (kStoreF32 only): partial sums into ws[split][M][N]
+    float* ws;
+    float* rhs;               // kApplyRhs: the solver's RHS (5 planes of rhs_npts values)
+    long long rhs_npts;
+    int rhs_rows;             // elements (rows beyond are padding)
+    float rhs_scale[5];
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -148,7 +157,9 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
     const int warp = t >> 5;
     const int m0 = blockIdx.x * BM;
     const int n0 = blockIdx.y * NT;
-    const int KB = g.K / BK;
+    const int ks = g.ksplit > 1 ? g.ksplit : 1;
+    const int KB = g.K / BK / ks;             // K blocks of this CTA's range
+    const int kb0 = (int)blockIdx.z * KB;
     constexpr uint32_t kCols = NT;  // fp32 accumulator: one column per N
 
     if (t == 0) {
@@ -169,7 +180,7 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
     const uint32_t tmem = s.tmem_base;
     const uint32_t idesc = instr_desc(BM, NT);
 
-    load_stage<NT>(g, s, 0, m0, n0, 0);
+    load_stage<NT>(g, s, 0, m0, n0, kb0);
     for (int kb = 0; kb < KB; ++kb) {
         const int st = kb % STAGES;
         // block kb has landed in stage st
@@ -206,7 +217,7 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
                 }
             }
             __syncthreads();
-            if (!s.failed) load_stage<NT>(g, s, nst, m0, n0, kb + 1);
+            if (!s.failed) load_stage<NT>(g, s, nst, m0, n0, kb0 + kb + 1);
         }
     }
     // all MMAs done: commit once more on the final barrier
@@ -221,13 +232,20 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
         ok = false;
         if (g.err) atomicExch(g.err, 1);
     }
+    ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
-        const int row = m0 + warp * 32 + (t & 31);
+        // Epilogue per 32-column chunk: the accumulator rows come out of TMEM
+        // one row per thread; row-major outputs go through a 32 x 32 shared
+        // staging tile (XOR-swizzled, in the now idle operand buffer) so that
+        // each store instruction writes one contiguous row segment.
+        const int lane = t & 31;
+        const int row0 = m0 + warp * 32;
+        float* stg = reinterpret_cast<float*>(s.a[0]) + warp * 1024;
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
-        for (int c0 = 0; c0 < NT; c0 += 16) {
-            uint32_t r[16];
+        for (int c0 = 0; c0 < NT; c0 += 32) {
+            uint32_t r[32];
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                 "[%16];"
@@ -235,26 +253,84 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
                   "=r"(r[15])
                 : "r"(lane_base + (uint32_t)c0));
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+                  "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+                  "=r"(r[30]), "=r"(r[31])
+                : "r"(lane_base + (uint32_t)(c0 + 16)));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             const int n = n0 + c0;
+            float v[32];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                float v = __uint_as_float(r[j]);
-                const size_t idx = (size_t)row * g.N + n + j;
-                if constexpr (EPI == kStoreF32) {
-                    if (g.bias) v += g.bias[n + j];
-                    g.out_f32[idx] = v;
-                } else if constexpr (EPI == kBiasGelu) {
-                    v += g.bias[n + j];
-                    g.out_f32[idx] = v;
-                    const __nv_bfloat16 a = __float2bfloat16_rn(gelu(v));
-                    g.out_bf[idx] = a;
-                    if (g.out_bfT) g.out_bfT[(size_t)(n + j) * g.M + row] = a;
-                } else {
-                    const __nv_bfloat16 d = __float2bfloat16_rn(v * gelu_grad(g.z_in[idx]));
-                    g.out_bf[idx] = d;
-                    if (g.out_bfT) g.out_bfT[(size_t)(n + j) * g.M + row] = d;
+            for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+            if constexpr (EPI == kGeluGrad) {
+                // z_in of this row chunk, read row by row (coalesced) through the staging tile
+#pragma unroll 4
+                for (int rr = 0; rr < 32; ++rr) stg[rr * 32 + (lane ^ rr)] = g.z_in[(size_t)(row0 + rr) * g.N + n + lane];
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] *= gelu_grad(stg[lane * 32 + (j ^ lane)]);
+                __syncwarp();
+            } else {
+                if (g.bias && !(EPI == kStoreF32 && ks > 1)) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] += g.bias[n + j];
                 }
+            }
+            // row-major fp32 output: C, the split-K partial, or z
+            if constexpr (EPI == kApplyRhs) {
+                // columns n..n+31 lie in one variable's 64-point block
+                const int var = n >> 6;
+                if (var < 5) {
+                    const float sc = g.rhs_scale[var];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j];
+                    __syncwarp();
+                    float* base = g.rhs + (size_t)var * g.rhs_npts + (n & 63) + lane;
+#pragma unroll 4
+                    for (int rr = 0; rr < 32; ++rr) {
+                        if (row0 + rr < g.rhs_rows) {
+                            float* q = base + (size_t)(row0 + rr) * 64;
+                            *q += sc * stg[rr * 32 + (lane ^ rr)];
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            if constexpr (EPI == kStoreF32 || EPI == kBiasGelu) {
+                // (z of a hidden layer is kept only for training: null at inference)
+                float* dst = EPI == kStoreF32 && ks > 1 ? g.ws + (size_t)blockIdx.z * g.M * g.N : g.out_f32;
+                if (dst) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j];
+                    __syncwarp();
+#pragma unroll 4
+                    for (int rr = 0; rr < 32; ++rr)
+                        dst[(size_t)(row0 + rr) * g.N + n + lane] = stg[rr * 32 + (lane ^ rr)];
+                    __syncwarp();
+                }
+            }
+            // bf16 outputs: gelu(z) or dz, row-major and (optionally) transposed
+            if constexpr (EPI == kBiasGelu || EPI == kGeluGrad) {
+                if constexpr (EPI == kBiasGelu) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = __bfloat162float(__float2bfloat16_rn(v[j]));
+                if (g.out_bfT) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) g.out_bfT[(size_t)(n + j) * g.M + row0 + lane] = __float2bfloat16_rn(v[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j];
+                __syncwarp();
+#pragma unroll 4
+                for (int rr = 0; rr < 32; ++rr)
+                    g.out_bf[(size_t)(row0 + rr) * g.N + n + lane] = __float2bfloat16_rn(stg[rr * 32 + (lane ^ rr)]);
+                __syncwarp();
             }
         }
     }
@@ -269,6 +345,7 @@ template <int NT>
 constexpr size_t gemm_smem_bytes() {
     return sizeof(Smem<NT>) + 1024;
 }
+
 
 }  // namespace mlp
 }  // namespace od

@@ -82,9 +82,30 @@ __device__ __forceinline__ int line_pt(int fp, int m) {
 
 // Face value from the four samples of a line; one fixed FMA chain so that the
 // two elements sharing a face compute bit-identical face states.
-template <class T>
-__device__ __forceinline__ T trace4(const T* q, const T* c) {
+template <class T, class CC>
+__device__ __forceinline__ T trace4(const T* q, const CC& c) {
     return fma(q[3], c[3], fma(q[2], c[2], fma(q[1], c[1], q[0] * c[0])));
+}
+
+// Face values at both ends of a line (trace4 with cL and with cR).
+template <class T, class CL, class CR>
+__device__ __forceinline__ void trace4_lr(const T* q, const CL& cL, const CR& cR, T& oL, T& oR) {
+    oL = trace4(q, cL);
+    oR = trace4(q, cR);
+}
+
+// r[a] = (sum_m D[a*4+m] q[m]) * s for a = 0..3 (the FR derivative along a
+// line). Paired f32 forms (FFMA2) of these loops measured 3% slower on B200:
+// the pairs cost operand moves and registers.
+template <class T, class DM>
+__device__ __forceinline__ void deriv4(const T* q, const DM& D, T s, T* r) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        T df = (T)0;
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) df = fma(D[a * 4 + mm], q[mm], df);
+        r[a] = df * s;
+    }
 }
 
 // neighbour across face (d, side) or -1 for a slip wall
@@ -197,6 +218,9 @@ struct alignas(16) SlotA {
 
 template <class S, class P, class C>
 struct StageAParams {
+    using S_t = S;
+    using P_t = P;
+    using C_t = C;
     const S* u_in;
     const S* u0;
     S* u_out;       // new state, or the RHS when phase B performs the RK combination
@@ -283,10 +307,10 @@ __device__ __forceinline__ void row_line_store(T* row, int l, int swz, const T* 
 }
 
 // P2-P4: one direction of the gradient / face-value pass for line l.
-template <class M, int FLUX, int D, class S, class P, class C>
-__device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, int l, int swz,
-                                          const long long nb0, const long long nb1, long long e, bool live,
-                                          P* oL, P* oR) {
+template <class M, int FLUX, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
+__device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, int swz, const long long nb0,
+                                          const long long nb1, long long e, bool live, P* oL, P* oR) {
+    using S = typename PA::S_t;
     const Mesh& m = A.m;
     P q[NV][4];
 #pragma unroll
@@ -294,8 +318,7 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
     P nL[NV], nR[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        oL[v] = trace4(q[v], A.tp.eL);
-        oR[v] = trace4(q[v], A.tp.eR);
+        trace4_lr(q[v], A.tp.eL, A.tp.eR, oL[v], oR[v]);
         const P refl = (v > 0 && v < 4) ? (P)-1.0 : (P)1.0;
         if (nb0 >= 0) {
             P w[4];
@@ -332,12 +355,10 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
         const C jr = (C)((P)0.5 * (nR[v] + oR[v]) - oR[v]);
         C qc[4] = {(C)q[v][0], (C)q[v][1], (C)q[v][2], (C)q[v][3]};
         C gv[4];
+        deriv4(qc, A.tc.D, jac, gv);
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            C der = (C)0;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) der = fma(A.tc.D[a * 4 + mm], qc[mm], der);
-            C gg = der * jac;
+            C gg = gv[a];
             gg += jl * A.tc.gL[a] * jac;
             gg += jr * A.tc.gR[a] * jac;
             if constexpr (sizeof(C) == 8) {
@@ -365,9 +386,9 @@ __device__ __forceinline__ void line_pass(const StageAParams<S, P, C>& A, SlotA<
 
 // Viscous part at one face point: j += 1/2 Fv_own; Fv_own (components 1..4)
 // to the face buffer for the neighbour's phase B.
-template <class M, int D, class S, class P, class C>
-__device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
-                                             int side, const P* qp, const C* gt, bool live) {
+template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
+__device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long long e, int l, int side,
+                                             const P* qp, const C* gt, bool live) {
     const int f = 2 * D + side;
     C praw;
     FaceState<C> s = make_face_state<M, C, P>(qp, praw);
@@ -385,8 +406,8 @@ __device__ __forceinline__ void viscous_face(const StageAParams<S, P, C>& A, Slo
 // The reference's y-face gradient slice multiplies with __fmul_rn, a float
 // intrinsic, also in its f64 build (rhs.cu:145-160): products and pair sums
 // in f32. Reproduced on request (kRefYSlice) for bit-level drop-in parity.
-template <class C>
-__device__ __forceinline__ C ref_y_slice(const C* w, const C* c) {
+template <class C, class CC>
+__device__ __forceinline__ C ref_y_slice(const C* w, const CC& c) {
     const float a = __fadd_rn(__fmul_rn((float)w[0], (float)c[0]), __fmul_rn((float)w[1], (float)c[1]));
     const float b = __fadd_rn(__fmul_rn((float)w[2], (float)c[2]), __fmul_rn((float)w[3], (float)c[3]));
     return (C)__fadd_rn(a, b);
@@ -394,8 +415,8 @@ __device__ __forceinline__ C ref_y_slice(const C* w, const C* c) {
 
 // P5: face values and face gradient along the D-line of thread l, viscous
 // flux at both faces of the line.
-template <class M, int D, class S, class P, class C>
-__device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long e, int l,
+template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
+__device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, long long e, int l,
                                                int swz, bool wall0, bool wall1, bool live, const P* tL,
                                                const P* tR) {
     if (wall0 && wall1) return;
@@ -414,8 +435,7 @@ __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, S
             gL[c] = ref_y_slice(w, A.tc.eL);
             gR[c] = ref_y_slice(w, A.tc.eR);
         } else {
-            gL[c] = trace4(w, A.tc.eL);
-            gR[c] = trace4(w, A.tc.eR);
+            trace4_lr(w, A.tc.eL, A.tc.eR, gL[c], gR[c]);
         }
     }
     // face values: kept in registers from the line pass (f32), else recomputed
@@ -428,8 +448,7 @@ __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, S
         } else {
             P w[4];
             row_line_load<D>(sm.u[v], l, swz, w);
-            qL[v] = trace4(w, A.tp.eL);
-            qR[v] = trace4(w, A.tp.eR);
+            trace4_lr(w, A.tp.eL, A.tp.eR, qL[v], qR[v]);
         }
     }
     if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live);
@@ -437,20 +456,14 @@ __device__ __forceinline__ void face_grad_pass(const StageAParams<S, P, C>& A, S
 }
 
 // P7: divergence of F_D along the line of thread l (times the Jacobian).
-template <int D, class C>
-__device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, const C* Dm, C jac) {
+template <int D, class C, class DM>
+__device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, const DM& Dm, C jac) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C w[4];
         row_line_load<D>(F + v * NE, l, swz, w);
         C r[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            C df = (C)0;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) df = fma(Dm[a * 4 + mm], w[mm], df);
-            r[a] = df * jac;
-        }
+        deriv4(w, Dm, jac, r);
         row_line_store<D>(out + v * NE, l, swz, r);
     }
 }
@@ -458,9 +471,10 @@ __device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, con
 // P8 of phase A for one live element: RHS = -div + forcing, own-face lifting
 // -(j_L g_L' + j_R g_R') jac, then the RK combination, or (deferred RK) the
 // unrounded RHS + own lift for phase B.
-template <class S, class P, class C>
-__device__ __forceinline__ void stage_a_update(const StageAParams<S, P, C>& A, SlotA<P, C>& sm, long long ec, int l,
-                                               int swz, const C* divy) {
+template <class PA, class P = typename PA::P_t, class C = typename PA::C_t>
+__device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, long long ec, int l, int swz,
+                                               const C* divy) {
+    using S = typename PA::S_t;
     const Mesh& m = A.m;
     const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
     const int px = sw(4 * l, swz);
@@ -509,9 +523,11 @@ __device__ __forceinline__ void stage_a_update(const StageAParams<S, P, C>& A, S
 
 // One tile of phase A: EPB elements starting at A.e0 + tile * EPB, LPE
 // threads each. Called by every thread of the block (it synchronises).
-template <class S, class P, class C, class M, int FLUX, int EPB>
-__device__ __forceinline__ void stage_a_tile(const StageAParams<S, P, C>& A, unsigned char* smem_raw,
-                                             long long tile) {
+template <class M, int FLUX, int EPB, class PA>
+__device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_raw, long long tile) {
+    using S = typename PA::S_t;
+    using P = typename PA::P_t;
+    using C = typename PA::C_t;
     const int l = threadIdx.x & (LPE - 1);
     const int es = threadIdx.x / LPE;
     const int swz = (es & 1) << 3;
@@ -593,17 +609,20 @@ __device__ __forceinline__ void stage_a_tile(const StageAParams<S, P, C>& A, uns
     __syncthreads();
 
     // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
-    if (live) stage_a_update<S, P, C>(A, sm, ec, l, swz, divy);
+    if (live) stage_a_update(A, sm, ec, l, swz, divy);
 }
 
 template <class S, class P, class C, class M, int FLUX, int EPB>
 __global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S, P, C> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    stage_a_tile<S, P, C, M, FLUX, EPB>(A, smem_raw, blockIdx.x);
+    stage_a_tile<M, FLUX, EPB>(A, smem_raw, blockIdx.x);
 }
 
 template <class S, class P, class C>
 struct StageBParams {
+    using S_t = S;
+    using P_t = P;
+    using C_t = C;
     S* u_out;
     const S* rhs;   // deferred RK: phase A's RHS
     const S* u_in;
@@ -638,8 +657,11 @@ __device__ __forceinline__ T ldf(const T* p) {
 // One tile of phase B: EPB elements starting at B.e0 + tile * EPB. COH: the
 // face buffers and the RHS were written by this same launch (a persistent
 // kernel after its grid barrier), so they are read through the coherent path.
-template <class S, class P, class C, int EPB, bool COH>
-__device__ __forceinline__ void stage_b_tile(const StageBParams<S, P, C>& B, long long tile) {
+template <int EPB, bool COH, class PB>
+__device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
+    using S = typename PB::S_t;
+    using P = typename PB::P_t;
+    using C = typename PB::C_t;
     const int l = threadIdx.x & (LPE - 1);
     const long long e = B.e0 + tile * EPB + threadIdx.x / LPE;
     const Mesh& m = B.m;
@@ -732,13 +754,15 @@ __device__ __forceinline__ void stage_b_tile(const StageBParams<S, P, C>& B, lon
 #pragma unroll
             for (int i = 0; i < 4; ++i) out[i] = cur[i] + B.rc * (P)acc[i];
         }
+        // stored per variable: holding all five (20 more registers) cut the
+        // occupancy and measured 20% slower
         stg4<S, P>(B.u_out + off, out);
     }
 }
 
 template <class S, class P, class C, int EPB>
 __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
-    stage_b_tile<S, P, C, EPB, false>(B, blockIdx.x);
+    stage_b_tile<EPB, false>(B, blockIdx.x);
 }
 
 }  // namespace od

@@ -194,7 +194,7 @@ def features_numpy(u, nx, ny, nz, lx, ly, lz, mean, scale):
             ch.append((d[1 + a][b] - q[1 + a] / rho * d[0][b]) / rho)
     ch = np.stack([c.reshape(nx * ny * nz, 64) for c in ch], axis=1)  # (e, c, p)
     ch = (ch - np.asarray(mean)[None, :, None]) / np.asarray(scale)[None, :, None]
-    return ch.reshape(nx * ny * nz, N_IN)
+    return np.clip(ch, -8.0, 8.0).reshape(nx * ny * nz, N_IN)
 
 
 # ---------------------------------------------------------------- device initial state
@@ -346,6 +346,7 @@ def generate_data(cfg, device=0, log=print):
     prf = torch.empty_like(uc)
     rc = torch.empty_like(uc)
     mean = scale = None
+    calib = {}
     row = 0
     t0 = time.perf_counter()
     dt = float(np.float32(cfg["dt_fine"]))
@@ -353,6 +354,8 @@ def generate_data(cfg, device=0, log=print):
         for si, seed in enumerate(seeds):
             u0 = _fine_ic(cfg, seed)
             set_state_device(fine, u0)
+            if si == len(seeds) - 1:
+                calib["u0"] = project(u0, nc, nc, nc, fac)
             del u0
             for k in range(nsnap):
                 fine.step(every, dt)
@@ -368,11 +371,16 @@ def generate_data(cfg, device=0, log=print):
                     h = features_numpy(uc.cpu().numpy(), nc, nc, nc, *cfg["box"], np.zeros(N_CHAN), np.ones(N_CHAN))
                     h = h.reshape(ne, N_CHAN, 64)
                     mean = h.mean(axis=(0, 2)).astype(np.float32)
-                    scale = np.maximum(h.std(axis=(0, 2)), 1e-6).astype(np.float32)
+                    # a floor of 1e-3 of the mean: density varies by ~1e-6 in the
+                    # training states, more in a coarse run
+                    scale = np.maximum(np.maximum(h.std(axis=(0, 2)), 1e-3 * np.abs(mean)), 1e-6).astype(np.float32)
                 features_device(uc, nc, cfg["box"], mean, scale, X[row:row + ne])
                 d = (prf - rc).view(5, ne, 64).permute(1, 0, 2).reshape(ne, N_OUT)
                 Traw[row:row + ne] = d
                 row += ne
+                if si == len(seeds) - 1 and k == nsnap - 1:
+                    calib["ref"] = uc.clone()
+                    calib["steps"] = every * nsnap
             log(f"seed {seed}: {nsnap} snapshots, {time.perf_counter() - t0:.1f} s")
     finally:
         fine.close()
@@ -383,7 +391,7 @@ def generate_data(cfg, device=0, log=print):
     del Traw, Tn
     torch.cuda.empty_cache()
     return {"X": X, "T": T, "mean": mean, "scale": scale, "out_scale": out_scale.astype(np.float32),
-            "rows_per_seed": nsnap * ne, "seeds": seeds, "gen_s": time.perf_counter() - t0}
+            "rows_per_seed": nsnap * ne, "seeds": seeds, "gen_s": time.perf_counter() - t0, "calib": calib}
 
 
 def train(data, cfg, device=0, log=print, net=None):
@@ -402,6 +410,7 @@ def train(data, cfg, device=0, log=print, net=None):
     steps_per_epoch = max(1, n_train // B)
     total_steps = cfg["epochs"] * steps_per_epoch
     hist = []
+    best = (float("inf"), None)
     t0 = time.perf_counter()
     step = 0
     for ep in range(cfg["epochs"]):
@@ -413,8 +422,48 @@ def train(data, cfg, device=0, log=print, net=None):
             step += 1
         val = validate(net, data, n_train) if n_train < n else float("nan")
         hist.append((ep, float(np.mean(losses)), val))
+        if not (val >= best[0]):
+            best = (val, net.get_params())
         log(f"epoch {ep}: train {np.mean(losses):.4f} val {val:.4f} ({time.perf_counter() - t0:.1f} s)")
-    return net, {"history": hist, "train_s": time.perf_counter() - t0, "steps": step}
+    if best[1] is not None:
+        net.set_params(best[1])
+    return net, {"history": hist, "train_s": time.perf_counter() - t0, "steps": step, "best_val": best[0]}
+
+
+def calibrate(net, data, cfg, device=0, log=print, alphas=(1.0, 0.5, 0.25, 0.125)):
+    """A posteriori gain of the correction: the coarse run of the last
+    training seed (the validation seed) with rhs += alpha * correction for
+    each alpha, compared with that seed's filtered fine state at the end of
+    the horizon; keeps the alpha with the smallest Reynolds-stress error
+    (alpha = 0, the plain solver, is the fallback)."""
+    cal = data["calib"]
+    nc = cfg["coarse"]
+    dt = cfg["dt_fine"] * cfg["fine"] / nc
+    steps = int(round(cal["steps"] * cfg["dt_fine"] / dt))
+    s = Solver(_params(nc, cfg, device))
+    try:
+        set_state_device(s, cal["ref"])
+        ref = _profiles(s)
+        results = []
+        for a in (0.0,) + tuple(alphas):
+            if a > 0:
+                net.set_scaling(data["mean"], data["scale"], a * data["out_scale"])
+                net.attach(s)
+            set_state_device(s, cal["u0"])
+            s.step(steps, float(np.float32(dt)))
+            s.sync()
+            err = _errors(_profiles(s), ref)
+            if a > 0:
+                Network.detach(s)
+            ok = np.isfinite(err["stress"]) and np.isfinite(err["mean_u"])
+            results.append((a, err))
+            log(f"calibration alpha {a}: {err}")
+        good = [(e["stress"], a) for a, e in results if np.isfinite(e["stress"])]
+        best = min(good)[1] if good else 0.0
+    finally:
+        s.close()
+    net.set_scaling(data["mean"], data["scale"], best * data["out_scale"])
+    return best, results
 
 
 def validate(net, data, start):

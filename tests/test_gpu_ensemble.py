@@ -10,7 +10,7 @@ import math
 import numpy as np
 import pytest
 
-from helpers import random_smooth, rel_l2
+from helpers import random_smooth
 from opendynamo_b200.forms.ensemble import Box, Ensemble, benchmark_boxes
 from opendynamo_b200.solver import Solver
 
@@ -28,9 +28,14 @@ def _states(boxes):
 
 
 def _close(got, want):
-    """f32 round-off: the two kernels differ in a few last bits."""
-    assert np.all(rel_l2(got, want) < 1e-7), rel_l2(got, want)
-    assert np.abs(got.astype(np.float64) - want).max() < 1e-6
+    """f32 round-off: the two kernels differ in a few last bits. Measured per
+    variable against the density's norm (rho*w of a Taylor-Green box is
+    round-off itself)."""
+    g = got.astype(np.float64).reshape(5, -1)
+    w = want.astype(np.float64).reshape(5, -1)
+    scale = np.maximum(np.linalg.norm(w, axis=1), np.linalg.norm(w[0]))
+    assert np.all(np.linalg.norm(g - w, axis=1) < 1e-7 * scale), np.linalg.norm(g - w, axis=1) / scale
+    assert np.abs(g - w).max() < 1e-6
 
 
 def _alone(boxes, states, steps):

@@ -1,5 +1,6 @@
 """The closure network's tcgen05 BF16 GEMM against an fp32 matmul of the
-same bf16 operands (torch, as the checker)."""
+same bf16 operands (torch, as the checker): every tile width (64 / 128 /
+256), one- and multi-block K, and split-K (few tiles, long K)."""
 
 import ctypes
 
@@ -11,7 +12,8 @@ from opendynamo_b200 import _native as N
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("M,Nn,K", [(128, 256, 64), (128, 128, 128), (256, 384, 896), (384, 256, 320),
-                                    (128, 512, 192)])
+                                    (128, 512, 192), (128, 64, 64), (13824, 256, 896), (8192, 384, 256),
+                                    (256, 896, 8192), (384, 256, 4096)])
 @pytest.mark.parametrize("bias", [False, True])
 def test_gemm_bf16_matches_fp32_matmul(M, Nn, K, bias):
     import torch
@@ -36,4 +38,6 @@ def test_gemm_rejects_bad_shapes():
     assert N.lib().od_gemm_bf16(100, 128, 64, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_void_p(1), None,
                                 None) == -1
     assert N.lib().od_gemm_bf16(128, 128, 60, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_void_p(1), None,
+                                None) == -1
+    assert N.lib().od_gemm_bf16(128, 100, 64, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_void_p(1), None,
                                 None) == -1
