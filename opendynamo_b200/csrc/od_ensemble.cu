@@ -125,6 +125,14 @@ struct EnsBoxStage {
     StageB B;
 };
 
+// Per-box parameters of the running stage in constant memory (ensembles of
+// up to kConstBoxes boxes): the stage code then reads them as it reads
+// kernel parameters in the single-box kernels, cached and known constant
+// across barriers. Copied in before every stage launch (a node of the step
+// graph), so ensembles on one device must not run concurrently.
+constexpr int kConstBoxes = 64;
+__constant__ EnsBoxStage c_boxes[kConstBoxes];
+
 __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -156,19 +164,6 @@ __device__ __forceinline__ bool grid_barrier(GridSync* g) {
     return ok != 0;
 }
 
-// box of global tile t (starts: nbox + 1 prefix sums)
-__device__ __forceinline__ int find_box(const long long* starts, int nbox, long long t) {
-    int lo = 0, hi = nbox - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (starts[mid] <= t)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
 template <class T>
 __device__ __forceinline__ void block_copy(T* dst, const T* src) {
     static_assert(sizeof(T) % 4 == 0, "word copy");
@@ -179,16 +174,18 @@ __device__ __forceinline__ void block_copy(T* dst, const T* src) {
 
 // 8 (EPB 4) or 16 (EPB 2) blocks per SM: 128 registers per thread, the
 // occupancy of the single-box phase-A kernel (shared memory bounds both).
-template <class M, int EPB>
+template <class M, int EPB, bool CP>
 __global__ void __launch_bounds__(LPE * EPB, 16 / EPB * 2) ensemble_stage_kernel(const EnsBoxStage* __restrict__ boxes, int nbox,
                                                                    const long long* __restrict__ start_a,
                                                                    const long long* __restrict__ start_b,
+                                                                   const int2* __restrict__ tile_map,
+                                                                   const int2* __restrict__ tile_map_b,
                                                                    GridSync* sync) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) StageA As;
-    __shared__ __align__(16) StageB Bs;
-    __shared__ int box_s;
     const long long G = gridDim.x;
+    // tile_map[t] = (box, tile inside the box); the entry of the next tile is
+    // loaded while the current one is processed
     // phase A: tiles blockIdx.x, +G, +2G, ... of all boxes. At any moment the
     // grid works on a window of consecutive tiles, as the waves of a single-box
     // launch do, so the neighbours' state read by one tile is still in L2 from
@@ -197,47 +194,57 @@ __global__ void __launch_bounds__(LPE * EPB, 16 / EPB * 2) ensemble_stage_kernel
     {
         const long long total = start_a[nbox];
         int cur = -1;
+        int2 info = blockIdx.x < total ? tile_map[blockIdx.x] : make_int2(0, 0);
         for (long long t = blockIdx.x; t < total; t += G) {
-            if (threadIdx.x == 0) box_s = find_box(start_a, nbox, t);
-            __syncthreads();
-            const int b = box_s;
-            if (b != cur) {
-                block_copy(&As, &boxes[b].A);
-                cur = b;
+            const int2 next = t + G < total ? tile_map[t + G] : info;
+            __syncthreads();  // the previous tile is done with the element slots (and As)
+            if constexpr (CP) {
+                od::stage_a_tile<M, od::kFluxRuntime, EPB>(c_boxes[info.x].A, smem_raw, info.y);
+            } else {
+                if (info.x != cur) {
+                    block_copy(&As, &boxes[info.x].A);
+                    cur = info.x;
+                    __syncthreads();
+                }
+                od::stage_a_tile<M, od::kFluxRuntime, EPB>(As, smem_raw, info.y);
             }
-            __syncthreads();
-            od::stage_a_tile<M, od::kFluxRuntime, EPB>(As, smem_raw, t - start_a[b]);
+            info = next;
         }
     }
     if (!grid_barrier(sync)) return;
-    // phase B, same order
+    // phase B, same order. Its tiles are short, so the parameters of every box
+    // are copied into the (now idle) element slots once, and the loop has no
+    // block synchronisation.
     {
         const long long total = start_b[nbox];
-        int cur = -1;
+        StageB* Bs = reinterpret_cast<StageB*>(smem_raw);
+        const bool in_smem = !CP && (size_t)nbox * sizeof(StageB) <= sizeof(SlotA<float, float>) * EPB;
+        if (in_smem) {
+            for (int b = 0; b < nbox; ++b) block_copy(&Bs[b], &boxes[b].B);
+            __syncthreads();
+        }
+        int2 info = blockIdx.x < total ? tile_map_b[blockIdx.x] : make_int2(0, 0);
         for (long long t = blockIdx.x; t < total; t += G) {
-            __syncthreads();
-            if (threadIdx.x == 0) box_s = find_box(start_b, nbox, t);
-            __syncthreads();
-            const int b = box_s;
-            if (b != cur) {
-                __syncthreads();
-                block_copy(&Bs, &boxes[b].B);
-                cur = b;
-                __syncthreads();
-            }
-            od::stage_b_tile<EPB, true>(Bs, t - start_b[b]);
+            const int2 next = t + G < total ? tile_map_b[t + G] : info;
+            if constexpr (CP)
+                od::stage_b_tile<EPB, true>(c_boxes[info.x].B, info.y);
+            else if (in_smem)
+                od::stage_b_tile<EPB, true>(Bs[info.x], info.y);
+            else
+                od::stage_b_tile<EPB, true>(boxes[info.x].B, info.y);
+            info = next;
         }
     }
 }
 
 template <class M, int EPB>
-void* kernel_ptr() {
-    return (void*)ensemble_stage_kernel<M, EPB>;
+void* kernel_ptr(bool cp) {
+    return cp ? (void*)ensemble_stage_kernel<M, EPB, true> : (void*)ensemble_stage_kernel<M, EPB, false>;
 }
 
-void* pick_kernel(bool fast, int epb) {
-    if (fast) return epb == 2 ? kernel_ptr<od::MathFast, 2>() : kernel_ptr<od::MathFast, 4>();
-    return epb == 2 ? kernel_ptr<od::MathIeee, 2>() : kernel_ptr<od::MathIeee, 4>();
+void* pick_kernel(bool fast, int epb, bool cp) {
+    if (fast) return epb == 2 ? kernel_ptr<od::MathFast, 2>(cp) : kernel_ptr<od::MathFast, 4>(cp);
+    return epb == 2 ? kernel_ptr<od::MathIeee, 2>(cp) : kernel_ptr<od::MathIeee, 4>(cp);
 }
 
 size_t dyn_smem(int epb) { return sizeof(SlotA<float, float>) * (size_t)epb; }
@@ -258,6 +265,8 @@ struct od_ensemble {
     EnsBoxStage* d_stage[3] = {nullptr, nullptr, nullptr};
     long long* d_start_a = nullptr;  // per EPB choice: rebuilt by set_shape
     long long* d_start_b = nullptr;
+    int2* d_tile_map = nullptr;      // (box, tile in box) of every phase-A tile (sized for 2 elements per tile)
+    int2* d_tile_map_b = nullptr;    // the same for the phase-B tiles
     GridSync* d_sync = nullptr;
     // shape
     int epb = 4, bps = 0, grid = 0;
@@ -355,14 +364,28 @@ int build_stage_params(od_ensemble* E) {
     cudaError_t c = cudaMemcpyToSymbol(c_tab, &ht, sizeof ht);
     if (c == cudaSuccess) c = cudaMemcpy(E->d_start_a, sa.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice);
     if (c == cudaSuccess) c = cudaMemcpy(E->d_start_b, sb.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice);
+    std::vector<int2> ta((size_t)sa[nb]), tb((size_t)sb[nb]);
+    for (int b = 0; b < nb; ++b) {
+        for (long long t = sa[b]; t < sa[b + 1]; ++t) ta[(size_t)t] = make_int2(b, (int)(t - sa[b]));
+        for (long long t = sb[b]; t < sb[b + 1]; ++t) tb[(size_t)t] = make_int2(b, (int)(t - sb[b]));
+    }
+    if (c == cudaSuccess) c = cudaMemcpy(E->d_tile_map, ta.data(), sizeof(int2) * ta.size(), cudaMemcpyHostToDevice);
+    if (c == cudaSuccess) c = cudaMemcpy(E->d_tile_map_b, tb.data(), sizeof(int2) * tb.size(), cudaMemcpyHostToDevice);
     if (c != cudaSuccess) return ecuda(E, c, "tile tables");
     return OD_OK;
 }
 
 cudaError_t launch_stage(od_ensemble* E, int s) {
-    void* fn = pick_kernel(E->fast, E->epb);
     int nbox = (int)E->box.size();
+    const bool cp = nbox <= kConstBoxes;
+    void* fn = pick_kernel(E->fast, E->epb, cp);
+    if (cp) {
+        cudaError_t c = cudaMemcpyToSymbolAsync(c_boxes, E->d_stage[s], sizeof(EnsBoxStage) * nbox, 0,
+                                                cudaMemcpyDeviceToDevice, E->stream);
+        if (c != cudaSuccess) return c;
+    }
     void* args[] = {(void*)&E->d_stage[s], (void*)&nbox, (void*)&E->d_start_a, (void*)&E->d_start_b,
+                    (void*)&E->d_tile_map, (void*)&E->d_tile_map_b,
                     (void*)&E->d_sync};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)E->grid);
@@ -386,7 +409,7 @@ void drop_graph(od_ensemble* E) {
 // set the launch shape; blocks_per_sm <= 0 = as many as are co-resident
 int apply_shape(od_ensemble* E, int epb, int bps, bool use_graph) {
     if (epb != 2 && epb != 4) return efail(E, OD_ERR_ARG, "elements per block must be 2 or 4");
-    void* fn = pick_kernel(E->fast, epb);
+    void* fn = pick_kernel(E->fast, epb, E->box.size() <= (size_t)kConstBoxes);
     cudaError_t c = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem(epb));
     if (c != cudaSuccess) return ecuda(E, c, "cudaFuncSetAttribute");
     int maxb = 0;
@@ -494,6 +517,10 @@ int od_ensemble_create(const od_box* boxes, int nbox, int device, int fast_math,
     for (int s = 0; s < 3 && c == cudaSuccess; ++s) c = cudaMalloc(&E->d_stage[s], sizeof(EnsBoxStage) * nbox);
     if (c == cudaSuccess) c = cudaMalloc(&E->d_start_a, sizeof(long long) * (nbox + 1));
     if (c == cudaSuccess) c = cudaMalloc(&E->d_start_b, sizeof(long long) * (nbox + 1));
+    long long max_tiles = 0;
+    for (int b = 0; b < nbox; ++b) max_tiles += (E->nelem[b] + 1) / 2;
+    if (c == cudaSuccess) c = cudaMalloc(&E->d_tile_map, sizeof(int2) * (size_t)max_tiles);
+    if (c == cudaSuccess) c = cudaMalloc(&E->d_tile_map_b, sizeof(int2) * (size_t)max_tiles);
     if (c == cudaSuccess) c = cudaMalloc(&E->d_sync, sizeof(GridSync));
     if (c != cudaSuccess) {
         *out = E;
@@ -520,6 +547,8 @@ void od_ensemble_destroy(od_ensemble* E) {
         if (E->d_stage[s]) cudaFree(E->d_stage[s]);
     if (E->d_start_a) cudaFree(E->d_start_a);
     if (E->d_start_b) cudaFree(E->d_start_b);
+    if (E->d_tile_map) cudaFree(E->d_tile_map);
+    if (E->d_tile_map_b) cudaFree(E->d_tile_map_b);
     if (E->d_sync) cudaFree(E->d_sync);
     if (E->pool) cudaFree(E->pool);
     if (E->stream) cudaStreamDestroy(E->stream);
@@ -600,7 +629,7 @@ int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t r
     cudaEventCreate(&e1);
     int rc = OD_OK;
     for (int epb : {2, 4}) {
-        void* fn = pick_kernel(E->fast, epb);
+        void* fn = pick_kernel(E->fast, epb, E->box.size() <= (size_t)kConstBoxes);
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem(epb));
         int maxb = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, LPE * epb, dyn_smem(epb));

@@ -202,7 +202,7 @@ __device__ __forceinline__ int sw(int p, int swz) { return p ^ (((p >> 3) & 4) |
 
 template <class P, class C>
 struct SlotBytes {
-    static constexpr int base = 15 * NE * (int)sizeof(C) + NV * NE * (int)sizeof(P) + 6 * NV * NF * (int)sizeof(C);
+    static constexpr int base = 15 * NE * (int)sizeof(C) + NV * NE * (int)sizeof(P) + 4 * NV * NF * (int)sizeof(C);
     static constexpr int words = base / 4;
     static constexpr int pad_words = ((16 - words % 32) + 32) % 32 == 0 ? 32 : ((16 - words % 32) + 32) % 32;
 };
@@ -212,7 +212,8 @@ template <class P, class C>
 struct alignas(16) SlotA {
     C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9, F_x rows 10-14; P7: div_z / div_x in place
     P u[NV][NE];          // state; P7: div_y (as C)
-    C j[6][NV][NF];       // face corrections without -1/2 Fv_nbr [face = 2d + side][var][face pt]
+    C j[4][NV][NF];       // y / z face corrections without -1/2 Fv_nbr [face - 2][var][face pt]; the x faces of
+                          // a line belong to its own thread and stay in registers
     float pad[SlotBytes<P, C>::pad_words];
 };
 
@@ -309,7 +310,8 @@ __device__ __forceinline__ void row_line_store(T* row, int l, int swz, const T* 
 // P2-P4: one direction of the gradient / face-value pass for line l.
 template <class M, int FLUX, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, int swz, const long long nb0,
-                                          const long long nb1, long long e, bool live, P* oL, P* oR) {
+                                          const long long nb1, long long e, bool live, P* oL, P* oR,
+                                          C (&jx)[2][NV]) {
     using S = typename PA::S_t;
     const Mesh& m = A.m;
     P q[NV][4];
@@ -379,8 +381,13 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, i
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        sm.j[2 * D][v][l] = j0[v];
-        sm.j[2 * D + 1][v][l] = j1[v];
+        if constexpr (D == 0) {
+            jx[0][v] = j0[v];
+            jx[1][v] = j1[v];
+        } else {
+            sm.j[2 * D - 2][v][l] = j0[v];
+            sm.j[2 * D - 1][v][l] = j1[v];
+        }
     }
 }
 
@@ -388,14 +395,19 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, i
 // to the face buffer for the neighbour's phase B.
 template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long long e, int l, int side,
-                                             const P* qp, const C* gt, bool live) {
+                                             const P* qp, const C* gt, bool live, C (&jx)[2][NV]) {
     const int f = 2 * D + side;
     C praw;
     FaceState<C> s = make_face_state<M, C, P>(qp, praw);
     C fv[NV];
     viscous_flux<D>(s, praw, gt, viscosity<M>(A.mu, A.suth, s), fv);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) sm.j[f][v][l] += (C)0.5 * fv[v];
+    for (int v = 0; v < NV; ++v) {
+        if constexpr (D == 0)
+            jx[side][v] += (C)0.5 * fv[v];
+        else
+            sm.j[f - 2][v][l] += (C)0.5 * fv[v];
+    }
     if (live) {
         C* out = A.fv + ((e * 6 + f) * 4) * NF + l;
 #pragma unroll
@@ -418,7 +430,7 @@ __device__ __forceinline__ C ref_y_slice(const C* w, const CC& c) {
 template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, long long e, int l,
                                                int swz, bool wall0, bool wall1, bool live, const P* tL,
-                                               const P* tR) {
+                                               const P* tR, C (&jx)[2][NV]) {
     if (wall0 && wall1) return;
     C gL[15], gR[15];
     const bool ref_y = D == 1 && sizeof(C) == 8 && (A.flags & kRefYSlice);
@@ -451,8 +463,8 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
             trace4_lr(w, A.tp.eL, A.tp.eR, qL[v], qR[v]);
         }
     }
-    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live);
-    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live);
+    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live, jx);
+    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live, jx);
 }
 
 // P7: divergence of F_D along the line of thread l (times the Jacobian).
@@ -473,7 +485,7 @@ __device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, con
 // unrounded RHS + own lift for phase B.
 template <class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, long long ec, int l, int swz,
-                                               const C* divy) {
+                                               const C* divy, const C (&jx)[2][NV]) {
     using S = typename PA::S_t;
     const Mesh& m = A.m;
     const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
@@ -485,11 +497,11 @@ __device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, lon
         ld4s(&sm.g[10 + v][px], dx);
         ld4s(&divy[v * NE + px], dy);
         ld4s(&sm.g[5 + v][px], dz);
-        ld4s(&sm.j[2][v][4 * lk], jy0);
-        ld4s(&sm.j[3][v][4 * lk], jy1);
-        ld4s(&sm.j[4][v][4 * lj], jz0);
-        ld4s(&sm.j[5][v][4 * lj], jz1);
-        const C jx0 = sm.j[0][v][l], jx1 = sm.j[1][v][l];
+        ld4s(&sm.j[0][v][4 * lk], jy0);
+        ld4s(&sm.j[1][v][4 * lk], jy1);
+        ld4s(&sm.j[2][v][4 * lj], jz0);
+        ld4s(&sm.j[3][v][4 * lj], jz1);
+        const C jx0 = jx[0][v], jx1 = jx[1][v];
         C rt[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -559,15 +571,16 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
 
     // ---- P2-P4: face values, gradient, interface fluxes per direction
     P tr[3][2][NV];   // own face values of this thread's lines (kept only for f32 state arithmetic)
-    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp, ec, live, tr[0][0], tr[0][1]);
-    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp, ec, live, tr[1][0], tr[1][1]);
-    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp, ec, live, tr[2][0], tr[2][1]);
+    C jx[2][NV];      // this x-line's x-face corrections
+    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp, ec, live, tr[0][0], tr[0][1], jx);
+    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp, ec, live, tr[1][0], tr[1][1], jx);
+    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp, ec, live, tr[2][0], tr[2][1], jx);
     __syncthreads();
 
     // ---- P5: viscous face fluxes of all six faces
-    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live, tr[0][0], tr[0][1]);
-    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live, tr[1][0], tr[1][1]);
-    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live, tr[2][0], tr[2][1]);
+    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live, tr[0][0], tr[0][1], jx);
+    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live, tr[1][0], tr[1][1], jx);
+    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live, tr[2][0], tr[2][1], jx);
     __syncthreads();
 
     // ---- P6: pointwise fluxes of the x-line's points (own points only; the
@@ -609,7 +622,7 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     __syncthreads();
 
     // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
-    if (live) stage_a_update(A, sm, ec, l, swz, divy);
+    if (live) stage_a_update(A, sm, ec, l, swz, divy, jx);
 }
 
 template <class S, class P, class C, class M, int FLUX, int EPB>
