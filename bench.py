@@ -46,10 +46,8 @@ BYTES_PER_DOF_STAGE = 40.0 / 3.0  # x sizeof(state): read u + write u' (stage 1)
 
 
 def _dist():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from opendynamo_b200 import replicas
+    return replicas.world()
 
 
 class ClockSampler:
@@ -152,14 +150,10 @@ def run_ours(args, world, rank, local):
     import torch
     from opendynamo_b200.solver import Solver, make_params
 
+    from opendynamo_b200 import replicas
     w = WORKLOAD
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        import datetime
-        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        dist = dist_mod
+    dist = replicas.init("nccl")
     u_host = build_state(np.float32)
     npts = w["nx"] * w["ny"] * w["nz"] * 64
     params = make_params(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"], w["lz"], w["flux"], w["y_wall"], w["prec"],
@@ -192,12 +186,9 @@ def run_ours(args, world, rank, local):
     barrier()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(ms, dist, f"cuda:{local}")
     stages = args.steps * RK_PER_STEP * 3
-    value = world * npts * stages / (ms / 1e3) / 1e9
+    value = replicas.job_throughput(npts * stages, ms / 1e3, world) / 1e9
 
     # ---- dominant kernel (phase A) timed live with events on the solver's stream
     solver.set_timing(True)
@@ -227,12 +218,8 @@ def run_ours(args, world, rank, local):
         solver.step(RK_PER_STEP, dt)
         assert lib.od_get_state(solver._ctx, ctypes.c_void_p(h_out.data_ptr()), solver.state_bytes) == 0
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * npts * stages / e2e_s / 1e9
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+    e2e_value = replicas.job_throughput(npts * stages, e2e_s, world) / 1e9
     final = h_out.numpy()
     finite = bool(np.isfinite(final).all())
 
@@ -271,8 +258,7 @@ def run_ours(args, world, rank, local):
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(u_host)
     solver.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    replicas.finish(dist)
     return out
 
 
