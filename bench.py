@@ -300,13 +300,14 @@ def run_ensemble_form(args, world, rank, local):
     import torch
     from opendynamo_b200.forms.ensemble import benchmark_boxes, compare_with_loop
     torch.cuda.set_device(local)
-    boxes = benchmark_boxes()
+    boxes = benchmark_boxes() if not args.mesh else benchmark_boxes(n_min=max(2, args.mesh // 4), n_max=args.mesh)
     steps = args.form_steps or 20
     res = compare_with_loop(boxes, steps=steps, warmup=args.warmup, device=local)
-    return {"metric": "aggregate Gdof*stage/s, 64-box ensemble (8^3-32^3, seed 7), f32",
+    lo, hi = (8, 32) if not args.mesh else (max(2, args.mesh // 4), args.mesh)
+    return {"metric": f"aggregate Gdof*stage/s, 64-box ensemble ({lo}^3-{hi}^3, seed 7), f32",
             "value": round(res["ensemble_gdof_stage_s"], 3), "unit": "Gdof*stage/s", "n_gpus": 1, "steps": steps,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic (TGV / tripped-channel boxes, seed 7)",
-            "config": {"workload": "64 boxes, log-uniform 8^3..32^3, Mach 0.05-0.3, Re 400-1600, Rusanov/SLAU2",
+            "config": {"workload": f"64 boxes, log-uniform {lo}^3..{hi}^3, Mach 0.05-0.3, Re 400-1600, Rusanov/SLAU2",
                        "form": "ensemble"},
             "loop_value": round(res["loop_gdof_stage_s"], 3), "study": res}
 
@@ -364,6 +365,48 @@ def run_closure_form(args, world, rank, local):
             "evaluation": ev, "normalisation": norm}
 
 
+def run_closure_step(args, world, rank, local):
+    """Cost of the learned closure inside the step: the coarse channel (24^3 by
+    default) stepped with and without the network attached (random weights,
+    output scaled to 1e-6 so the flow stays the plain one). CUDA events on the
+    solver's stream."""
+    if rank != 0:
+        return None
+    import torch
+    from opendynamo_b200.forms import closure as CL
+    from opendynamo_b200.solver import Solver, make_params
+    torch.cuda.set_device(local)
+    n = args.mesh or 24
+    steps = args.form_steps or 50
+    box = (2 * math.pi, 2.0, math.pi)
+    dt = 8e-4 * 24 / n
+    p = make_params(n, n, n, *box, u_real="f32", mu=0.2 / 3000, device=local)
+    u = CL.channel_state_device(n, *box, 0.2, 0.01, 16, 1)
+    net = CL.Network(max_rows=n ** 3, device=local)
+    net.set_params(CL.init_params(np.random.default_rng(0)))
+    net.set_scaling(np.zeros(14), np.ones(14), np.full(5, 1e-6, np.float32))
+    out = {}
+    with Solver(p) as s:
+        CL.set_state_device(s, u)
+        for name, attach in (("closure", True), ("plain", False)):
+            if attach:
+                net.attach(s)
+            else:
+                CL.Network.detach(s)
+            s.step(args.warmup, float(np.float32(dt)))
+            s.sync()
+            out[name] = CL._timed_steps(s, steps, dt) / steps
+    net.close()
+    npts = n ** 3 * 64
+    return {"metric": f"closure step cost, channel {n}^3 (ms per SSP-RK3 step)", "value": round(out["closure"], 4),
+            "unit": "ms/step", "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "f32 solver / bf16 network", "data": "synthetic (channel trip IC, random network)",
+            "config": {"workload": f"channel {n}^3, SLAU2, per-stage features + 4 tcgen05 GEMMs",
+                       "form": "closure-step"},
+            "plain_ms_per_step": round(out["plain"], 4),
+            "closure_gdof_stage_s": round(npts * 3 / (out["closure"] / 1e3) / 1e9, 3)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -371,7 +414,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="plain", choices=["plain", "precision", "ensemble", "closure"],
+    ap.add_argument("--form", default="plain", choices=["plain", "precision", "ensemble", "closure", "closure-step"],
                     help="plain: the headline 48^3 bench; precision: the precision-form study")
     ap.add_argument("--mesh", type=int, default=0, help="elements per axis of a --form run (0 = its default)")
     ap.add_argument("--form-steps", type=int, default=0, help="RK3 steps of a --form run (0 = its default)")
@@ -392,6 +435,8 @@ def main():
         out = run_ensemble_form(args, world, rank, local)
     elif args.form == "closure":
         out = run_closure_form(args, world, rank, local)
+    elif args.form == "closure-step":
+        out = run_closure_step(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if out is not None and rank == 0:

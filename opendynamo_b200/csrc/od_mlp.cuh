@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
             for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
             if constexpr (EPI == kGeluGrad) {
                 // z_in of this row chunk, read row by row (coalesced) through the staging tile
-#pragma unroll 4
+#pragma unroll
                 for (int rr = 0; rr < 32; ++rr) stg[rr * 32 + (lane ^ rr)] = g.z_in[(size_t)(row0 + rr) * g.N + n + lane];
                 __syncwarp();
 #pragma unroll
@@ -289,13 +289,14 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
                     for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j];
                     __syncwarp();
                     float* base = g.rhs + (size_t)var * g.rhs_npts + (n & 63) + lane;
-#pragma unroll 4
-                    for (int rr = 0; rr < 32; ++rr) {
-                        if (row0 + rr < g.rhs_rows) {
-                            float* q = base + (size_t)(row0 + rr) * 64;
-                            *q += sc * stg[rr * 32 + (lane ^ rr)];
-                        }
-                    }
+                    // all 32 row segments loaded first (one memory round trip), then updated
+                    float cur[32];
+#pragma unroll
+                    for (int rr = 0; rr < 32; ++rr)
+                        cur[rr] = row0 + rr < g.rhs_rows ? base[(size_t)(row0 + rr) * 64] : 0.f;
+#pragma unroll
+                    for (int rr = 0; rr < 32; ++rr)
+                        if (row0 + rr < g.rhs_rows) base[(size_t)(row0 + rr) * 64] = cur[rr] + sc * stg[rr * 32 + (lane ^ rr)];
                     __syncwarp();
                 }
             }
