@@ -156,7 +156,7 @@ int od_timing(od_ctx* ctx, double* ms_phase_a, double* ms_phase_b, long long* n_
  * The kernels' only scratch, the per-face viscous and interface fluxes, lives
  * in one static device array of OD_NOALLOC_SCRATCH_BYTES per GPU (held until
  * exit), which limits the mesh to OD_NOALLOC_SCRATCH_BYTES /
- * (624 * sizeof(compute type)) elements (6721 in f32 compute, 3360 in f64);
+ * (432 * sizeof(compute type)) elements (9709 in f32 compute, 4854 in f64);
  * larger meshes return
  * OD_ERR_SCRATCH. All calls share the array: calls whose kernels overlap on
  * the GPU race, so order them on one stream. The first call on a device looks
@@ -225,6 +225,41 @@ int od_state_load(const char* path, void* planes_out, size_t bytes, int expect_u
 
 /* Message of this thread's last state-file failure. */
 const char* od_state_error(void);
+
+/* ------------------------------------------------------------------------
+ * Post-processing: the ParaView conversion of scripts/h5_to_xdmf.py.
+ * ------------------------------------------------------------------------ */
+
+/* Point fields of a state on the device (enqueued on `stream`): planes = 5
+ * device planes of the state type, out = 7 device f32 arrays of
+ * (4nx) x (4ny) x (4nz) points, row-major with z fastest — the reference's
+ * to_tensor order (scripts/h5_to_xdmf.py:35-44): rho, rhou, rhov, rhow, E,
+ * vel = sqrt(rhou^2 + rhov^2 + rhow^2) / max(rho, 1e-30) and
+ * p = max(1e-7, 0.4 (E - 0.5 (rhou^2 + rhov^2 + rhow^2) / max(rho, 1e-30)))
+ * (h5_to_xdmf.py:74-79), in f32 after rounding f64 planes to f32, with the
+ * script's operation order. */
+int od_point_fields(const void* planes, int u_f64, int nx, int ny, int nz, float* out, void* stream);
+
+/* Point-field file: group /data with nfields 3-D f32 datasets n0 x n1 x n2
+ * (row-major), chunk min(chunk, n) per dimension, compression as
+ * od_state_save ("gzip4" in the conversion). */
+int od_fields_save(const char* path, const float* fields, int nfields, const char* const* names,
+                   long long n0, long long n1, long long n2, int chunk, const char* compression);
+
+/* The .xmf text of a converted file (3DRectMesh of npx x npy x npz cells,
+ * VXVYVZ axes linspace(0, L, n + 1), the 7 point fields as cell attributes
+ * from <h5_name>:/data/<field>), h5_to_xdmf.py:87-123. Writes at most len
+ * bytes (NUL-terminated) and returns the full length, or < 0. */
+long long od_xdmf_text(char* buf, size_t len, const char* h5_name, int npx, int npy, int npz, double lx,
+                       double ly, double lz, unsigned long long step, double t);
+
+/* Convert one state file: <stem>.pv.h5 (the 7 point fields, chunks of 48,
+ * shuffle + gzip 4) and <stem>.xmf beside it, computed on the current
+ * device. out_h5 / out_xmf (may be null) receive the two paths. Returns 0,
+ * or < 0 with the message in err.
+ * Replaces: process() of scripts/h5_to_xdmf.py:47-143. */
+int od_xdmf_convert(const char* src, char* out_h5, size_t out_h5_len, char* out_xmf, size_t out_xmf_len,
+                    char* err, int err_len);
 
 /* ------------------------------------------------------------------------
  * Run driver: the reference's run loop (src/solver.rs:139-374, 745-818) on

@@ -32,6 +32,7 @@ EXPORTS = (
     "od_mlp_create", "od_mlp_destroy", "od_mlp_last_error", "od_mlp_param_count", "od_mlp_set_params",
     "od_mlp_get_params", "od_mlp_forward", "od_mlp_gradients", "od_mlp_train_step", "od_mlp_set_scaling",
     "od_attach_closure", "od_project", "od_closure_features", "od_f32_to_bf16",
+    "od_point_fields", "od_fields_save", "od_xdmf_text", "od_xdmf_convert",
 )
 
 
@@ -153,6 +154,12 @@ def lib() -> ctypes.CDLL:
         "od_project": (ci, [vp, ci, ci, ci, ci, ci, vp, ci, vp]),
         "od_closure_features": (ci, [vp, ci, ci, ci, ci, cd, cd, cd, vp, vp, vp, vp]),
         "od_f32_to_bf16": (ci, [vp, vp, ctypes.c_longlong, vp]),
+        "od_point_fields": (ci, [vp, ci, ci, ci, ci, vp, vp]),
+        "od_fields_save": (ci, [ctypes.c_char_p, vp, ci, ctypes.POINTER(ctypes.c_char_p), ctypes.c_longlong,
+                                ctypes.c_longlong, ctypes.c_longlong, ci, ctypes.c_char_p]),
+        "od_xdmf_text": (ctypes.c_longlong, [ctypes.c_char_p, sz, ctypes.c_char_p, ci, ci, ci, cd, cd, cd,
+                                             ctypes.c_ulonglong, cd]),
+        "od_xdmf_convert": (ci, [ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_char_p, sz, ctypes.c_char_p, ci]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

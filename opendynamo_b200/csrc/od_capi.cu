@@ -398,7 +398,7 @@ int od_create(const od_params* p, od_ctx** out) {
         }
     }
     // viscous face fluxes [elem][6][4][16] + minus-face interface fluxes [elem][3][5][16]
-    const size_t fv_bytes = (size_t)nelem * (6 * 4 + 3 * 5) * 16 * (c->fns.c_double ? 8 : 4);
+    const size_t fv_bytes = (size_t)nelem * od::kFaceWords * (c->fns.c_double ? 8 : 4);
     e = cudaMalloc(&c->fv, fv_bytes);
     if (e != cudaSuccess) {
         *out = c;

@@ -313,7 +313,7 @@ int build_stage_params(od_ensemble* E) {
             A.u0 = s == 0 ? nullptr : E->U[0][b];
             A.u_out = E->rhs[b];
             A.fv = E->fv[b];
-            A.fi = E->fv[b] + E->nelem[b] * 6 * 4 * NF;
+            A.fi = E->fv[b] + E->nelem[b] * od::kFvWords;
             A.m.nx = x.nx;
             A.m.ny = x.ny;
             A.m.nz = x.nz;
@@ -510,7 +510,7 @@ int od_ensemble_create(const od_box* boxes, int nbox, int device, int fast_math,
         E->nelem.push_back(ne);
         off[b] = total;
         const size_t st = (size_t)ne * NE * 5 * sizeof(float);
-        total += 4 * align(st) + align((size_t)ne * (6 * 4 + 3 * 5) * NF * sizeof(float));
+        total += 4 * align(st) + align((size_t)ne * od::kFaceWords * sizeof(float));
     }
     c = cudaMalloc(&E->pool, total);
     if (c == cudaSuccess) c = cudaMemset(E->pool, 0, total);

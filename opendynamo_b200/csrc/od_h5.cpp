@@ -443,22 +443,28 @@ Buf symtab_msg(const GroupAddrs& g) {
     return m;
 }
 
-// chunk B-tree (rank 1): leaves of up to 2K chunks, internal levels above
+// chunk B-tree: leaves of up to 2K chunks, internal levels above. Keys hold
+// the chunk's size (leaves), filter mask 0 and its element offsets per
+// dimension plus a trailing 0 for the element-size dimension; the key after
+// the last child is the last chunk's offsets advanced by one chunk in every
+// dimension (rank 1: the element offset one past the last chunk).
 uint64_t write_chunk_btree(FileWriter& w, const std::vector<uint64_t>& addr, const std::vector<uint32_t>& csize,
-                           uint64_t chunk_elems) {
-    const size_t key_size = 4 + 4 + 8 * 2;
+                           const std::vector<std::vector<uint64_t>>& offs, const std::vector<uint64_t>& cdims) {
+    const size_t rank = cdims.size();
+    const size_t key_size = 4 + 4 + 8 * (rank + 1);
     const size_t node_size = 24 + (2 * ISTORE_K + 1) * key_size + 2 * ISTORE_K * 8;
     struct Node {
         uint64_t addr;
-        uint64_t first, last_end;  // element offsets spanned
+        std::vector<uint64_t> first, last_end;  // offsets spanned
     };
-    std::vector<Node> level;
+    auto advance = [&](const std::vector<uint64_t>& o) {
+        std::vector<uint64_t> r = o;
+        for (size_t d = 0; d < rank; ++d) r[d] += cdims[d];
+        return r;
+    };
     std::vector<uint64_t> children = addr;
-    std::vector<uint64_t> starts(addr.size()), ends(addr.size());
-    for (size_t i = 0; i < addr.size(); ++i) {
-        starts[i] = i * chunk_elems;
-        ends[i] = (i + 1) * chunk_elems;
-    }
+    std::vector<std::vector<uint64_t>> starts = offs, ends(addr.size());
+    for (size_t i = 0; i < addr.size(); ++i) ends[i] = advance(offs[i]);
     int lvl = 0;
     std::vector<uint32_t> sizes = csize;
     while (true) {
@@ -476,13 +482,13 @@ uint64_t write_chunk_btree(FileWriter& w, const std::vector<uint64_t>& addr, con
             for (size_t i = b; i < e; ++i) {
                 n.u32(lvl == 0 ? sizes[i] : 0);
                 n.u32(0);
-                n.u64(starts[i]);
+                for (size_t d = 0; d < rank; ++d) n.u64(starts[i][d]);
                 n.u64(0);
                 n.u64(children[i]);
             }
             n.u32(0);
             n.u32(0);
-            n.u64(ends[e - 1]);
+            for (size_t d = 0; d < rank; ++d) n.u64(ends[e - 1][d]);
             n.u64(0);
             w.place(na, n);
             next.push_back({na, starts[b], ends[e - 1]});
@@ -500,16 +506,26 @@ uint64_t write_chunk_btree(FileWriter& w, const std::vector<uint64_t>& addr, con
     }
 }
 
-uint64_t write_dataset(FileWriter& w, const uint8_t* data, size_t n_elems, int es, const Compression& cmp) {
+// Dataset of float elements (es = 4 or 8) with dimensions `dims` (rank 1 to
+// 3, row-major data). "none" is contiguous; otherwise chunked with chunk
+// dimensions `cdims` (edge chunks are stored whole, zero-padded, as libhdf5
+// does) and the compression's filter pipeline.
+uint64_t write_dataset(FileWriter& w, const uint8_t* data, const std::vector<uint64_t>& dims,
+                       const std::vector<uint64_t>& cdims, int es, const Compression& cmp) {
     Buf dspace, dtype, layout, fill, filters;
     const bool chunked = cmp.kind != Comp::None;
+    const size_t rank = dims.size();
+    if (rank < 1 || rank > 3 || (chunked && cdims.size() != rank)) throw H5Error("unsupported dataset rank");
+    size_t n_elems = 1;
+    for (auto d : dims) n_elems *= d;
     dspace.u8(1);
-    dspace.u8(1);
+    dspace.u8((uint8_t)rank);
     dspace.u8(chunked ? 1 : 0);
     dspace.u8(0);
     dspace.u32(0);
-    dspace.u64(n_elems);
-    if (chunked) dspace.u64(n_elems);
+    for (auto d : dims) dspace.u64(d);
+    if (chunked)
+        for (auto d : dims) dspace.u64(d);
     dtype_float(dtype, es);
     fill.u8(2);
     fill.u8(chunked ? 3 : 2);  // incremental / late allocation
@@ -525,8 +541,36 @@ uint64_t write_dataset(FileWriter& w, const uint8_t* data, size_t n_elems, int e
         layout.u64(data_addr);
         layout.u64(bytes);
     } else {
-        const size_t chunk = std::min(n_elems, CHUNK_ELEMS);
-        const size_t nchunks = (n_elems + chunk - 1) / chunk;
+        // chunk grid, row-major (the B-tree's key order)
+        std::vector<uint64_t> ng(rank);
+        size_t nchunks = 1, chunk = 1;
+        for (size_t d = 0; d < rank; ++d) {
+            if (cdims[d] == 0 || cdims[d] > dims[d]) throw H5Error("chunk larger than the dataset");
+            ng[d] = (dims[d] + cdims[d] - 1) / cdims[d];
+            nchunks *= ng[d];
+            chunk *= cdims[d];
+        }
+        std::vector<std::vector<uint64_t>> offs(nchunks, std::vector<uint64_t>(rank));
+        for (size_t c = 0; c < nchunks; ++c) {
+            size_t r = c;
+            for (size_t d = rank; d-- > 0;) {
+                offs[c][d] = (r % ng[d]) * cdims[d];
+                r /= ng[d];
+            }
+        }
+        // gather one chunk (zero padding outside the dataset)
+        auto gather = [&](size_t c, uint8_t* raw) {
+            const auto& o = offs[c];
+            const uint64_t d1 = rank > 1 ? dims[rank - 2] : 1, d2 = dims[rank - 1];
+            const uint64_t k0 = rank > 2 ? cdims[0] : 1, k1 = rank > 1 ? cdims[rank - 2] : 1, k2 = cdims[rank - 1];
+            const uint64_t o0 = rank > 2 ? o[0] : 0, o1 = rank > 1 ? o[rank - 2] : 0, o2 = o[rank - 1];
+            const uint64_t d0 = rank > 2 ? dims[0] : 1;
+            const uint64_t run = std::min<uint64_t>(k2, d2 - o2);
+            for (uint64_t a = 0; a < k0 && o0 + a < d0; ++a)
+                for (uint64_t b = 0; b < k1 && o1 + b < d1; ++b)
+                    std::memcpy(raw + ((a * k1 + b) * k2) * es, data + (((o0 + a) * d1 + o1 + b) * d2 + o2) * es,
+                                run * es);
+        };
         std::vector<uint64_t> addrs;
         std::vector<uint32_t> sizes;
         // chunks are independent: encode them on up to kEncodeThreads threads
@@ -534,10 +578,8 @@ uint64_t write_dataset(FileWriter& w, const uint8_t* data, size_t n_elems, int e
         std::vector<std::string> errs(nchunks);
         auto encode = [&](size_t c) {
             try {
-                const size_t off = c * chunk;
-                const size_t cnt = std::min(chunk, n_elems - off);
                 std::vector<uint8_t> raw(chunk * es, 0), tmp(chunk * es);
-                std::memcpy(raw.data(), data + off * es, cnt * es);
+                gather(c, raw.data());
                 if (cmp.kind == Comp::Gzip) {
                     shuffle(raw.data(), tmp.data(), raw.size(), (size_t)es);
                     enc[c] = deflate_bytes(tmp, cmp.level);
@@ -566,12 +608,12 @@ uint64_t write_dataset(FileWriter& w, const uint8_t* data, size_t n_elems, int e
             sizes.push_back((uint32_t)enc[c].size());
             std::vector<uint8_t>().swap(enc[c]);
         }
-        const uint64_t bt = write_chunk_btree(w, addrs, sizes, chunk);
+        const uint64_t bt = write_chunk_btree(w, addrs, sizes, offs, cdims);
         layout.u8(3);
         layout.u8(2);
-        layout.u8(2);
+        layout.u8((uint8_t)(rank + 1));
         layout.u64(bt);
-        layout.u32((uint32_t)chunk);
+        for (auto k : cdims) layout.u32((uint32_t)k);
         layout.u32((uint32_t)es);
         filters.u8(1);
         if (cmp.kind == Comp::Gzip) {
@@ -737,6 +779,47 @@ int fail(const std::string& s, int code = -5) {
     return code;
 }
 
+// Root object header with `rmsgs`, superblock v0, then the file written
+// atomically (path.tmp renamed over path). Returns 0 or fail().
+int finish_file(FileWriter& w, const GroupAddrs& rg, const std::vector<std::pair<uint16_t, Buf>>& rmsgs,
+                const char* path) {
+    Buf roh = object_header(rmsgs);
+    const uint64_t root_ohdr = w.alloc(roh.size());
+    w.place(root_ohdr, roh);
+    w.f.pad8();
+    Buf sb;
+    const uint8_t sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
+    sb.raw(sig, 8);
+    sb.u8(0);
+    sb.u8(0);
+    sb.u8(0);
+    sb.u8(0);
+    sb.u8(0);
+    sb.u8(8);
+    sb.u8(8);
+    sb.u8(0);
+    sb.u16(GROUP_LEAF_K);
+    sb.u16(GROUP_INTERNAL_K);
+    sb.u32(0);
+    sb.u64(0);
+    sb.u64(UNDEF);
+    sb.u64(w.f.size());
+    sb.u64(UNDEF);
+    sym_entry(sb, 0, root_ohdr, 1, rg.btree, rg.heap);
+    w.place(0, sb);
+    std::string tmp = std::string(path) + ".tmp";
+    FILE* fp = std::fopen(tmp.c_str(), "wb");
+    if (!fp) return fail(std::string("cannot open ") + tmp + " for writing");
+    const size_t wr = std::fwrite(w.f.b.data(), 1, w.f.size(), fp);
+    const int cl = std::fclose(fp);
+    if (wr != w.f.size() || cl != 0) {
+        std::remove(tmp.c_str());
+        return fail(std::string("short write to ") + tmp);
+    }
+    if (std::rename(tmp.c_str(), path) != 0) return fail(std::string("cannot rename to ") + path);
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -754,7 +837,8 @@ int od_state_save(const char* path, const void* planes, int u_f64, int nx, int n
         w.f.zeros(96);  // superblock, patched at the end
         uint64_t ds_addr[5];
         for (int v = 0; v < 5; ++v)
-            ds_addr[v] = write_dataset(w, (const uint8_t*)planes + (size_t)v * npts * es, npts, es, cmp);
+            ds_addr[v] = write_dataset(w, (const uint8_t*)planes + (size_t)v * npts * es, {(uint64_t)npts},
+                                       {(uint64_t)std::min(npts, CHUNK_ELEMS)}, es, cmp);
         std::vector<Child> dkids;
         for (int v = 0; v < 5; ++v) dkids.push_back({VAR_NAMES[v], ds_addr[v], false, 0, 0});
         GroupAddrs dg = write_group_index(w, dkids);
@@ -772,41 +856,39 @@ int od_state_save(const char* path, const void* planes, int u_f64, int nx, int n
         for (int i = 0; i < 4; ++i)
             rmsgs.push_back({0x000C, attribute(f64n[i], [](Buf& b) { dtype_float(b, 8); }, &f64v[i], 8)});
         rmsgs.push_back({0x000C, attribute("u_real", dtype_str3, u_f64 ? "f64" : "f32", 3)});
-        Buf roh = object_header(rmsgs);
-        const uint64_t root_ohdr = w.alloc(roh.size());
-        w.place(root_ohdr, roh);
-        w.f.pad8();
-        Buf sb;
-        const uint8_t sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
-        sb.raw(sig, 8);
-        sb.u8(0);
-        sb.u8(0);
-        sb.u8(0);
-        sb.u8(0);
-        sb.u8(0);
-        sb.u8(8);
-        sb.u8(8);
-        sb.u8(0);
-        sb.u16(GROUP_LEAF_K);
-        sb.u16(GROUP_INTERNAL_K);
-        sb.u32(0);
-        sb.u64(0);
-        sb.u64(UNDEF);
-        sb.u64(w.f.size());
-        sb.u64(UNDEF);
-        sym_entry(sb, 0, root_ohdr, 1, rg.btree, rg.heap);
-        w.place(0, sb);
-        std::string tmp = std::string(path) + ".tmp";
-        FILE* fp = std::fopen(tmp.c_str(), "wb");
-        if (!fp) return fail(std::string("cannot open ") + tmp + " for writing");
-        const size_t wr = std::fwrite(w.f.b.data(), 1, w.f.size(), fp);
-        const int cl = std::fclose(fp);
-        if (wr != w.f.size() || cl != 0) {
-            std::remove(tmp.c_str());
-            return fail(std::string("short write to ") + tmp);
+        return finish_file(w, rg, rmsgs, path);
+    } catch (const std::exception& e) {
+        return fail(e.what());
+    }
+}
+
+// Point-field file: group /data with nfields 3-D f32 datasets (row-major
+// n0 x n1 x n2), no root attributes (the layout of the reference's ParaView
+// companion file, scripts/h5_to_xdmf.py:130-141).
+int od_fields_save(const char* path, const float* fields, int nfields, const char* const* names, long long n0,
+                   long long n1, long long n2, int chunk, const char* compression) {
+    try {
+        if (!path || !fields || !names || nfields <= 0 || n0 <= 0 || n1 <= 0 || n2 <= 0 || chunk <= 0)
+            return fail("invalid arguments", -1);
+        const Compression cmp = parse_compression(compression);
+        const std::vector<uint64_t> dims = {(uint64_t)n0, (uint64_t)n1, (uint64_t)n2};
+        std::vector<uint64_t> cdims(3);
+        for (int d = 0; d < 3; ++d) cdims[d] = std::min<uint64_t>((uint64_t)chunk, dims[d]);
+        const size_t n = (size_t)n0 * n1 * n2;
+        FileWriter w;
+        w.f.zeros(96);  // superblock, patched at the end
+        std::vector<Child> dkids;
+        for (int v = 0; v < nfields; ++v) {
+            if (!names[v] || !*names[v]) return fail("empty field name", -1);
+            const uint64_t a = write_dataset(w, (const uint8_t*)(fields + (size_t)v * n), dims, cdims, 4, cmp);
+            dkids.push_back({names[v], a, false, 0, 0});
         }
-        if (std::rename(tmp.c_str(), path) != 0) return fail(std::string("cannot rename to ") + path);
-        return 0;
+        GroupAddrs dg = write_group_index(w, dkids);
+        Buf doh = object_header({{0x0011, symtab_msg(dg)}});
+        const uint64_t data_ohdr = w.alloc(doh.size());
+        w.place(data_ohdr, doh);
+        GroupAddrs rg = write_group_index(w, {{"data", data_ohdr, true, dg.btree, dg.heap}});
+        return finish_file(w, rg, {{0x0011, symtab_msg(rg)}}, path);
     } catch (const std::exception& e) {
         return fail(e.what());
     }

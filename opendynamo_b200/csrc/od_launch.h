@@ -15,6 +15,12 @@ enum StageFlags : int {
     kRefYSlice = 16, // f64 compute: round the y-face gradient traces as the reference's __fmul_rn does
 };
 
+// Face-flux scratch per element, in compute-type words: the viscous fluxes
+// of the three plus faces ([dir 3][var 1..4][face pt 16]) followed by the
+// minus-face records ([dir 3][var 5][face pt 16]) F_I - 1/2 Fv_own.
+constexpr int kFvWords = 3 * 4 * 16;
+constexpr int kFaceWords = kFvWords + 3 * 5 * 16;
+
 // FR operator tables in double (the host computes them once, as
 // src/fr_math.rs:107-142 does, then each launch casts to its own types).
 struct TablesD {
@@ -25,7 +31,7 @@ struct StageLaunch {
     const void* u_in;
     const void* u0;      // null on stage 1 / single RHS evaluations
     void* u_out;
-    void* fv;            // viscous face buffer
+    void* fv;            // face-flux scratch (kFaceWords per element)
     void* rhs;           // RHS buffer of the deferred RK combination (null otherwise)
     int nx, ny, nz, y_wall;
     long long nelem;

@@ -72,7 +72,7 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.u0 = (const S*)L.u0;
     A.u_out = (S*)(L.rhs ? L.rhs : L.u_out);
     A.fv = (C*)L.fv;
-    A.fi = (C*)L.fv + L.nelem * 6 * 4 * NF;
+    A.fi = (C*)L.fv + L.nelem * kFvWords;
     A.m.nx = L.nx;
     A.m.ny = L.ny;
     A.m.nz = L.nz;

@@ -68,7 +68,7 @@ extern "C" int od_rhs_noalloc(const od_params* p, const void* d_state, void* d_r
     if (d_state == d_rhs) return OD_ERR_ARG;
     // viscous face fluxes (6 faces x 4 components) and minus-face interface
     // fluxes (3 faces x 5 components), 16 points each, per element
-    const size_t scratch = (size_t)nelem * (6 * 4 + 3 * 5) * 16 * (c_double ? 8 : 4);
+    const size_t scratch = (size_t)nelem * od::kFaceWords * (c_double ? 8 : 4);
     if (scratch > (size_t)OD_NOALLOC_SCRATCH_BYTES) return OD_ERR_SCRATCH;
 
     int prev = 0;

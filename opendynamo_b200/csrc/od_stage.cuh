@@ -15,10 +15,12 @@
 //        slip-wall mirror rhs.cu:111-114), corrected gradient along the line
 //        (rhs.cu:373-461); at the minus face of the line the interface flux
 //        F_I is solved once for both sides (j = F_I - Fe_own here, F_I kept
-//        in the face buffer for the minus neighbour); at the plus face
-//        j = -Fe_own (slip wall: j = [0,0,p_w,0,0] - Fe, complete)
+//        in registers); at the plus face j = -Fe_own (slip wall:
+//        j = [0,0,p_w,0,0] - Fe, complete)
 //   P5  x / y / z faces: gradient at the face (11 components), own viscous
-//        flux Fv; j += 1/2 Fv_own; Fv_own -> face buffer for the neighbour
+//        flux Fv; j += 1/2 Fv_own; to the face buffer for the neighbours:
+//        F_I - 1/2 Fv_own at the minus faces (all the minus neighbour still
+//        needs at its plus face), Fv_own at the plus faces
 //   P6  x-threads: pointwise Euler - viscous fluxes of their 4 points
 //        (rhs.cu:229-266) -> smem
 //   P7  divergence along x, y, z lines
@@ -29,8 +31,9 @@
 //   (Fe_own - Fv_own), is then complete except for the terms that belong to
 //   the neighbour: F_I at the plus faces and -1/2 Fv_nbr at every non-wall
 //   face.
-// Phase B — reads those from the face buffer records of the +x/+y/+z and
-// -x/-y/-z neighbours and adds their lifted contribution. With an f32 state
+// Phase B — reads those from the face buffer records of the +x/+y/+z
+// neighbours (F_I - 1/2 Fv_nbr) and -x/-y/-z neighbours (Fv_nbr) and adds
+// their lifted contribution. With an f32 state
 // phase A stores the unrounded RHS instead of the new state and phase B
 // performs the RK combination, so the state is rounded once per stage:
 // phase B's increments are often below half an f32 ulp of E and rho*u, and
@@ -225,8 +228,8 @@ struct StageAParams {
     const S* u_in;
     const S* u0;
     S* u_out;       // new state, or the RHS when phase B performs the RK combination
-    C* fv;          // [elem][face 6][var 4][face pt 16]: own viscous face flux, components 1..4
-    C* fi;          // [elem][dir 3][var 5][face pt 16]: interface flux of the element's minus faces
+    C* fv;          // [elem][dir 3][var 4][face pt 16]: own viscous flux (components 1..4) at the plus faces
+    C* fi;          // [elem][dir 3][var 5][face pt 16]: F_I - 1/2 Fv_own at the minus faces
     Mesh m;
     Tab<P> tp;
     Tab<C> tc;
@@ -310,8 +313,7 @@ __device__ __forceinline__ void row_line_store(T* row, int l, int swz, const T* 
 // P2-P4: one direction of the gradient / face-value pass for line l.
 template <class M, int FLUX, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, int swz, const long long nb0,
-                                          const long long nb1, long long e, bool live, P* oL, P* oR,
-                                          C (&jx)[2][NV]) {
+                                          const long long nb1, P* oL, P* oR, C (&jx)[2][NV], C* fi) {
     using S = typename PA::S_t;
     const Mesh& m = A.m;
     P q[NV][4];
@@ -370,15 +372,11 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, i
         }
         row_line_store<D>(sm.g[3 * v + D], l, swz, gv);
     }
-    // inviscid parts at the two faces of this line
-    C j0[NV], j1[NV], fi[NV];
+    // inviscid parts at the two faces of this line; F_I stays in registers
+    // until the minus face's viscous flux is known (P5)
+    C j0[NV], j1[NV];
     minus_face<M, FLUX, D, P, C>(oL, nL, nb0 < 0, j0, fi, A.flux);
     plus_face<M, D, P, C>(oR, nb1 < 0, j1);
-    if (live && nb0 >= 0) {
-        C* out = A.fi + ((e * 3 + D) * NV) * NF + l;
-#pragma unroll
-        for (int v = 0; v < NV; ++v) out[v * NF] = fi[v];
-    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         if constexpr (D == 0) {
@@ -391,11 +389,13 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, i
     }
 }
 
-// Viscous part at one face point: j += 1/2 Fv_own; Fv_own (components 1..4)
-// to the face buffer for the neighbour's phase B.
+// Viscous part at one face point: j += 1/2 Fv_own; to the face buffer for
+// the neighbour's phase B: F_I - 1/2 Fv_own at a minus face (fi: the
+// interface flux solved in the line pass), Fv_own (components 1..4) at a
+// plus face.
 template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long long e, int l, int side,
-                                             const P* qp, const C* gt, bool live, C (&jx)[2][NV]) {
+                                             const P* qp, const C* gt, bool live, C (&jx)[2][NV], const C* fi) {
     const int f = 2 * D + side;
     C praw;
     FaceState<C> s = make_face_state<M, C, P>(qp, praw);
@@ -408,8 +408,14 @@ __device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long 
         else
             sm.j[f - 2][v][l] += (C)0.5 * fv[v];
     }
-    if (live) {
-        C* out = A.fv + ((e * 6 + f) * 4) * NF + l;
+    if (!live) return;
+    if (side == 0) {
+        C* out = A.fi + ((e * 3 + D) * NV) * NF + l;
+        out[0] = fi[0];
+#pragma unroll
+        for (int v = 1; v < NV; ++v) out[v * NF] = fi[v] - (C)0.5 * fv[v];
+    } else {
+        C* out = A.fv + ((e * 3 + D) * 4) * NF + l;
 #pragma unroll
         for (int v = 1; v < NV; ++v) out[(v - 1) * NF] = fv[v];
     }
@@ -430,7 +436,7 @@ __device__ __forceinline__ C ref_y_slice(const C* w, const CC& c) {
 template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, long long e, int l,
                                                int swz, bool wall0, bool wall1, bool live, const P* tL,
-                                               const P* tR, C (&jx)[2][NV]) {
+                                               const P* tR, C (&jx)[2][NV], const C* fi) {
     if (wall0 && wall1) return;
     C gL[15], gR[15];
     const bool ref_y = D == 1 && sizeof(C) == 8 && (A.flags & kRefYSlice);
@@ -463,8 +469,8 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
             trace4_lr(w, A.tp.eL, A.tp.eR, qL[v], qR[v]);
         }
     }
-    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live, jx);
-    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live, jx);
+    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live, jx, fi);
+    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live, jx, fi);
 }
 
 // P7: divergence of F_D along the line of thread l (times the Jacobian).
@@ -572,15 +578,16 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     // ---- P2-P4: face values, gradient, interface fluxes per direction
     P tr[3][2][NV];   // own face values of this thread's lines (kept only for f32 state arithmetic)
     C jx[2][NV];      // this x-line's x-face corrections
-    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp, ec, live, tr[0][0], tr[0][1], jx);
-    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp, ec, live, tr[1][0], tr[1][1], jx);
-    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp, ec, live, tr[2][0], tr[2][1], jx);
+    C fi[3][NV];      // interface fluxes at the minus faces of this thread's lines
+    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp, tr[0][0], tr[0][1], jx, fi[0]);
+    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp, tr[1][0], tr[1][1], jx, fi[1]);
+    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp, tr[2][0], tr[2][1], jx, fi[2]);
     __syncthreads();
 
-    // ---- P5: viscous face fluxes of all six faces
-    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live, tr[0][0], tr[0][1], jx);
-    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live, tr[1][0], tr[1][1], jx);
-    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live, tr[2][0], tr[2][1], jx);
+    // ---- P5: viscous face fluxes of all six faces, face records
+    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live, tr[0][0], tr[0][1], jx, fi[0]);
+    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live, tr[1][0], tr[1][1], jx, fi[1]);
+    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live, tr[2][0], tr[2][1], jx, fi[2]);
     __syncthreads();
 
     // ---- P6: pointwise fluxes of the x-line's points (own points only; the
@@ -651,8 +658,8 @@ struct StageBParams {
 };
 
 // Phase B: the neighbour-dependent part of the face corrections,
-//   plus faces:  j += F_I (solved by the plus neighbour) - 1/2 Fv_nbr
-//   minus faces: j += -1/2 Fv_nbr
+//   plus faces:  j += F_I - 1/2 Fv_nbr (the plus neighbour's minus-face record)
+//   minus faces: j += -1/2 Fv_nbr (the minus neighbour's plus-face record)
 // lifted with -(j g') jac (rk.cu:12-25) over the element's non-wall faces and
 // added to the new state (times rc), or (deferred RK) folded into
 // u_out = ra*u0 + rb*u_in + rc*(RHS + lift). 16 threads per element, each the
@@ -691,7 +698,7 @@ __device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C acc[4] = {(C)0, (C)0, (C)0, (C)0};
-        // interface fluxes of the plus faces: the plus neighbour's minus-face record
+        // plus faces: the plus neighbours' minus-face records F_I - 1/2 Fv
         {
             const C f0 = ldf<COH>(B.fi + ((nxp * 3 + 0) * NV + v) * NF + l);
 #pragma unroll
@@ -712,35 +719,26 @@ __device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
             for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
         }
         if (v > 0) {
-            // viscous: the neighbour's record of the shared face is its opposite side
+            // minus faces: the minus neighbours' viscous fluxes at their plus faces
             const int q = v - 1;
             {
-                const C a0 = ldf<COH>(B.fv + ((nxm * 6 + 1) * 4 + q) * NF + l);
-                const C a1 = ldf<COH>(B.fv + ((nxp * 6 + 0) * 4 + q) * NF + l);
+                const C a0 = ldf<COH>(B.fv + ((nxm * 3 + 0) * 4 + q) * NF + l);
 #pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, fma(hx * B.tc.gR[i], a1, acc[i]));
+                for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, acc[i]);
             }
             if (nym >= 0) {
                 C w[4];
-                ld4s(B.fv + ((nym * 6 + 3) * 4 + q) * NF + 4 * lk, w);
+                ld4s(B.fv + ((nym * 3 + 1) * 4 + q) * NF + 4 * lk, w);
                 const C c = hy * B.tc.gL[lj];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
             }
-            if (nyp >= 0) {
+            {
                 C w[4];
-                ld4s(B.fv + ((nyp * 6 + 2) * 4 + q) * NF + 4 * lk, w);
-                const C c = hy * B.tc.gR[lj];
+                ld4s(B.fv + ((nzm * 3 + 2) * 4 + q) * NF + 4 * lj, w);
+                const C c = hz * B.tc.gL[lk];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
-            }
-            {
-                C w0[4], w1[4];
-                ld4s(B.fv + ((nzm * 6 + 5) * 4 + q) * NF + 4 * lj, w0);
-                ld4s(B.fv + ((nzp * 6 + 4) * 4 + q) * NF + 4 * lj, w1);
-                const C c0 = hz * B.tc.gL[lk], c1 = hz * B.tc.gR[lk];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i] = fma(c0, w0[i], fma(c1, w1[i], acc[i]));
             }
         }
         const long long off = v * m.npts + e * NE + 4 * l;

@@ -133,8 +133,12 @@ class Walker:
         for t, body in self.messages(ohdr):
             if t == 0x01:
                 ver, rank, flags = body[0], body[1], body[2]
-                assert ver == 1 and rank == 1
-                info["n"] = struct.unpack_from("<Q", body, 8)[0]
+                assert ver == 1 and 1 <= rank <= 3
+                dims = struct.unpack_from(f"<{rank}Q", body, 8)
+                if flags & 1:
+                    assert struct.unpack_from(f"<{rank}Q", body, 8 + 8 * rank) == dims, "fixed size"
+                info["dims"] = dims
+                info["n"] = int(np.prod(dims))
             elif t == 0x03:
                 assert body[0] == 0x11, "float class, version 1"
                 info["size"] = struct.unpack_from("<I", body, 4)[0]
@@ -147,9 +151,11 @@ class Walker:
                 if body[1] == 1:
                     info["addr"], info["bytes"] = struct.unpack_from("<QQ", body, 2)
                 else:
-                    assert body[2] == 2
+                    nd = body[2]
                     info["btree"] = struct.unpack_from("<Q", body, 3)[0]
-                    info["chunk"], info["esize"] = struct.unpack_from("<II", body, 11)
+                    *cd, info["esize"] = struct.unpack_from(f"<{nd}I", body, 11)
+                    info["cdims"] = tuple(cd)
+                    info["chunk"] = int(np.prod(cd))
             elif t == 0x0B:
                 assert body[0] == 1
                 nf = body[1]
@@ -162,27 +168,74 @@ class Walker:
                     info["filters"].append((fid, cv))
         return info
 
-    def chunks(self, btree):
-        """[(element offset, address, size, mask, key position)] of a rank-1 chunk index."""
+    def chunks(self, btree, rank=1):
+        """[(element offset, address, size, mask, key position)] of a chunk
+        index; the offset is a tuple of `rank` element offsets for rank > 1.
+        Checks that the keys are increasing (row-major) and that every node's
+        closing key lies beyond its last child."""
         out = []
-        self._chunk_node(btree, out)
+        self._chunk_node(btree, out, rank)
+        for a, b in zip(out, out[1:]):
+            ka = a[0] if rank > 1 else (a[0],)
+            kb = b[0] if rank > 1 else (b[0],)
+            assert ka < kb, "chunk keys in row-major order"
         return out
 
-    def _chunk_node(self, addr, out):
+    def _chunk_node(self, addr, out, rank):
         assert self.b[addr:addr + 4] == b"TREE" and self.b[addr + 4] == 1
         level = self.b[addr + 5]
         used = struct.unpack_from("<H", self.b, addr + 6)[0]
+        ksz = 8 + 8 * (rank + 1)
         p = addr + 24
+        first = len(out)
         for i in range(used):
-            size, mask, off0, off1 = struct.unpack_from("<IIQQ", self.b, p)
-            child = struct.unpack_from("<Q", self.b, p + 24)[0]
-            assert off1 == 0
+            size, mask = struct.unpack_from("<II", self.b, p)
+            offs = struct.unpack_from(f"<{rank + 1}Q", self.b, p + 8)
+            child = struct.unpack_from("<Q", self.b, p + ksz)[0]
+            assert offs[-1] == 0
             if level:
-                self._chunk_node(child, out)
+                self._chunk_node(child, out, rank)
             else:
                 assert child + size <= self.eof
-                out.append((off0, child, size, mask, p))
-            p += 32
+                out.append((offs[0] if rank == 1 else tuple(offs[:rank]), child, size, mask, p))
+            p += ksz + 8
+        closing = struct.unpack_from(f"<{rank + 1}Q", self.b, p + 8)[:rank]
+        last = out[-1][0] if rank > 1 else (out[-1][0],)
+        assert len(out) > first and tuple(closing) > tuple(last), "closing key beyond the last child"
+
+    def _decode(self, info, raw):
+        es = info["size"]
+        for k, (fid, cv) in reversed(list(enumerate(info["filters"]))):
+            if info.get("mask", 0) & (1 << k):
+                continue
+            if fid == 1:
+                raw = zlib.decompress(raw)
+            elif fid == 2:
+                raw = _unshuffle(raw, es)
+            elif fid == 32001:
+                raw = blosc_decode(raw)
+            else:
+                raise AssertionError(f"filter {fid}")
+        return raw
+
+    def read_array(self, ohdr):
+        """A float dataset of rank 1 to 3 as a numpy array of its dims."""
+        info = self.dataset(ohdr)
+        es, dims = info["size"], info["dims"]
+        dt = np.float32 if es == 4 else np.float64
+        if info["layout"] == 1:
+            return np.frombuffer(self.b[info["addr"]:info["addr"] + info["n"] * es], dtype=dt).reshape(dims).copy()
+        rank = len(dims)
+        cd = info["cdims"]
+        out = np.zeros(dims, dt)
+        for off, addr, size, mask, _ in self.chunks(info["btree"], rank):
+            off = off if rank > 1 else (off,)
+            raw = self._decode(dict(info, mask=mask), self.b[addr:addr + size])
+            assert len(raw) == int(np.prod(cd)) * es, "whole chunks"
+            blk = np.frombuffer(raw, dtype=dt).reshape(cd)
+            sl = tuple(slice(o, min(o + c, d)) for o, c, d in zip(off, cd, dims))
+            out[sl] = blk[tuple(slice(0, s.stop - s.start) for s in sl)]
+        return out
 
     def read_plane(self, ohdr):
         info = self.dataset(ohdr)

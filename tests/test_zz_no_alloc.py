@@ -66,7 +66,7 @@ def test_rhs_noalloc_matches_od_rhs_twice(prec):
 @pytest.mark.gpu
 def test_rhs_noalloc_rejects_meshes_beyond_the_scratch():
     import torch
-    n = 24  # 13824 elements > 16 MiB / (624 * 4 bytes)
+    n = 24  # 13824 elements > 16 MiB / (432 * 4 bytes)
     params = make_params(n, n, n, *BOX, "slau2", True, "f32")
     d_state = torch.zeros(n ** 3 * 64 * 5, dtype=torch.float32, device="cuda:0")
     d_out = torch.empty_like(d_state)
