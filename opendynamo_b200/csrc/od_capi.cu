@@ -557,7 +557,7 @@ void* od_stream(od_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int od_launches_per_step(const od_ctx* c) {
     if (!c) return 0;
-    return 3 * 2;
+    return 3 * 2 * (c->slabs > 1 && !c->hook ? c->slabs : 1);
 }
 
 int od_set_pipeline_slabs(od_ctx* c, int slabs) {
