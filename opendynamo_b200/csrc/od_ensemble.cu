@@ -86,6 +86,7 @@ struct StageA {
     float* fi;
     od::Mesh m;
     CTab tp, tc;
+    od::ScaledTab<float> sc;
     float jac[3];
     float ra, rb, rc;
     float mu, forcing, suth;
@@ -290,6 +291,14 @@ int ecuda(od_ensemble* e, cudaError_t c, const char* what) {
 // RK stage parameters of every box for the current shape
 int build_stage_params(od_ensemble* E) {
     const od::TablesD tab = od::host_fr_tables();
+    od::Tab<float> tables_f;
+    for (int i = 0; i < 16; ++i) tables_f.D[i] = (float)tab.D[i];
+    for (int i = 0; i < 4; ++i) {
+        tables_f.eL[i] = (float)tab.eL[i];
+        tables_f.eR[i] = (float)tab.eR[i];
+        tables_f.gL[i] = (float)tab.gL[i];
+        tables_f.gR[i] = (float)tab.gR[i];
+    }
     const int nb = (int)E->box.size();
     std::vector<EnsBoxStage> h(nb);
     std::vector<long long> sa(nb + 1, 0), sb(nb + 1, 0);
@@ -323,6 +332,7 @@ int build_stage_params(od_ensemble* E) {
             const double L3[3] = {x.lx, x.ly, x.lz};
             const int n3[3] = {x.nx, x.ny, x.nz};
             for (int d = 0; d < 3; ++d) A.jac[d] = 2.0f / ((float)L3[d] / (float)n3[d]);
+            A.sc = od::scale_tab<float>(tables_f, A.jac);
             A.ra = ra[s];
             A.rb = rb[s];
             A.rc = rc[s];
@@ -353,15 +363,7 @@ int build_stage_params(od_ensemble* E) {
         cudaError_t c = cudaMemcpy(E->d_stage[s], h.data(), sizeof(EnsBoxStage) * nb, cudaMemcpyHostToDevice);
         if (c != cudaSuccess) return ecuda(E, c, "stage parameters");
     }
-    od::Tab<float> ht;
-    for (int i = 0; i < 16; ++i) ht.D[i] = (float)tab.D[i];
-    for (int i = 0; i < 4; ++i) {
-        ht.eL[i] = (float)tab.eL[i];
-        ht.eR[i] = (float)tab.eR[i];
-        ht.gL[i] = (float)tab.gL[i];
-        ht.gR[i] = (float)tab.gR[i];
-    }
-    cudaError_t c = cudaMemcpyToSymbol(c_tab, &ht, sizeof ht);
+    cudaError_t c = cudaMemcpyToSymbol(c_tab, &tables_f, sizeof tables_f);
     if (c == cudaSuccess) c = cudaMemcpy(E->d_start_a, sa.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice);
     if (c == cudaSuccess) c = cudaMemcpy(E->d_start_b, sb.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice);
     std::vector<int2> ta((size_t)sa[nb]), tb((size_t)sb[nb]);

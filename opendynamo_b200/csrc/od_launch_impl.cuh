@@ -82,6 +82,7 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.tp = cast_tab<P>(L.tab);
     A.tc = cast_tab<C>(L.tab);
     for (int d = 0; d < 3; ++d) A.jac[d] = (C)L.jac[d];
+    A.sc = scale_tab<C>(A.tc, A.jac);
     A.ra = (P)L.ra;
     A.rb = (P)L.rb;
     A.rc = (P)L.rc;

@@ -67,6 +67,30 @@ struct Tab {
     T gR[4];   // Radau g_R'(x_a)
 };
 
+// The operators of each direction scaled by its Jacobian 2/h, so that the
+// corrected gradient, the divergence and the lifting are pure FMA chains:
+// d[dir][a*4+m] = D[a*4+m] jac[dir], gl / gr[dir][a] = g_L' / g_R'(x_a) jac[dir]
+// (products rounded in T).
+template <class T>
+struct ScaledTab {
+    T d[3][16];
+    T gl[3][4];
+    T gr[3][4];
+};
+
+template <class T, class TabT>
+__host__ ScaledTab<T> scale_tab(const TabT& t, const T* jac) {
+    ScaledTab<T> r;
+    for (int dir = 0; dir < 3; ++dir) {
+        for (int i = 0; i < 16; ++i) r.d[dir][i] = (T)(t.D[i] * jac[dir]);
+        for (int a = 0; a < 4; ++a) {
+            r.gl[dir][a] = (T)(t.gL[a] * jac[dir]);
+            r.gr[dir][a] = (T)(t.gR[a] * jac[dir]);
+        }
+    }
+    return r;
+}
+
 struct Mesh {
     int nx, ny, nz, y_wall;
     long long nelem, npts;
@@ -97,17 +121,17 @@ __device__ __forceinline__ void trace4_lr(const T* q, const CL& cL, const CR& cR
     oR = trace4(q, cR);
 }
 
-// r[a] = (sum_m D[a*4+m] q[m]) * s for a = 0..3 (the FR derivative along a
-// line). Paired f32 forms (FFMA2) of these loops measured 3% slower on B200:
-// the pairs cost operand moves and registers.
+// r[a] = sum_m D[a*4+m] q[m] for a = 0..3 (the FR derivative along a line,
+// D already scaled by the Jacobian). Paired f32 forms (FFMA2) of these loops
+// measured 3% slower on B200: the pairs cost operand moves and registers.
 template <class T, class DM>
-__device__ __forceinline__ void deriv4(const T* q, const DM& D, T s, T* r) {
+__device__ __forceinline__ void deriv4(const T* q, const DM& D, T* r) {
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-        T df = (T)0;
+        T df = D[a * 4] * q[0];
 #pragma unroll
-        for (int mm = 0; mm < 4; ++mm) df = fma(D[a * 4 + mm], q[mm], df);
-        r[a] = df * s;
+        for (int mm = 1; mm < 4; ++mm) df = fma(D[a * 4 + mm], q[mm], df);
+        r[a] = df;
     }
 }
 
@@ -233,6 +257,7 @@ struct StageAParams {
     Mesh m;
     Tab<P> tp;
     Tab<C> tc;
+    ScaledTab<C> sc;
     C jac[3];
     P ra, rb, rc;
     C mu, forcing;
@@ -351,20 +376,18 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, i
             nR[v] = oR[v] * refl;
         }
     }
-    // corrected gradient along the line (BR1)
-    const C jac = A.jac[D];
+    // corrected gradient along the line (BR1): jl g_L' + jr g_R' + D q, all
+    // scaled by the Jacobian, as one FMA chain per point
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         const C jl = (C)((P)0.5 * (nL[v] + oL[v]) - oL[v]);
         const C jr = (C)((P)0.5 * (nR[v] + oR[v]) - oR[v]);
-        C qc[4] = {(C)q[v][0], (C)q[v][1], (C)q[v][2], (C)q[v][3]};
         C gv[4];
-        deriv4(qc, A.tc.D, jac, gv);
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            C gg = gv[a];
-            gg += jl * A.tc.gL[a] * jac;
-            gg += jr * A.tc.gR[a] * jac;
+            C gg = fma(jr, A.sc.gr[D][a], jl * A.sc.gl[D][a]);
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) gg = fma(A.sc.d[D][a * 4 + mm], (C)q[v][mm], gg);
             if constexpr (sizeof(C) == 8) {
                 if (A.flags & kRoundQ) gg = (C)(float)gg;
             }
@@ -473,15 +496,16 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
     if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live, jx, fi);
 }
 
-// P7: divergence of F_D along the line of thread l (times the Jacobian).
+// P7: divergence of F_D along the line of thread l (Dm: the Jacobian-scaled
+// derivative of direction D).
 template <int D, class C, class DM>
-__device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, const DM& Dm, C jac) {
+__device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, const DM& Dm) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C w[4];
         row_line_load<D>(F + v * NE, l, swz, w);
         C r[4];
-        deriv4(w, Dm, jac, r);
+        deriv4(w, Dm, r);
         row_line_store<D>(out + v * NE, l, swz, r);
     }
 }
@@ -516,10 +540,13 @@ __device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, lon
             if constexpr (sizeof(C) == 8) {
                 if (A.flags & kRoundRhs) rvol = (C)(float)rvol;
             }
-            const C cx = -(jx0 * A.tc.gL[i] * A.jac[0]) - (jx1 * A.tc.gR[i] * A.jac[0]);
-            const C cy = -(jy0[i] * A.tc.gL[lj] * A.jac[1]) - (jy1[i] * A.tc.gR[lj] * A.jac[1]);
-            const C cz = -(jz0[i] * A.tc.gL[lk] * A.jac[2]) - (jz1[i] * A.tc.gR[lk] * A.jac[2]);
-            rt[i] = rvol + (cx + cy + cz);
+            // lifting -(j_L g_L' + j_R g_R') jac of the six faces (rk.cu:12-25)
+            C r = fma(-jx0, A.sc.gl[0][i], rvol);
+            r = fma(-jx1, A.sc.gr[0][i], r);
+            r = fma(-jy0[i], A.sc.gl[1][lj], r);
+            r = fma(-jy1[i], A.sc.gr[1][lj], r);
+            r = fma(-jz0[i], A.sc.gl[2][lk], r);
+            rt[i] = fma(-jz1[i], A.sc.gr[2][lk], r);
         }
         S* dst = A.u_out + v * m.npts + ec * NE + 4 * l;
         if (defer) {
@@ -623,9 +650,9 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
 
     // ---- P7: divergences: x in place (rows 10-14), y -> state region, z in place (rows 5-9)
     C* divy = reinterpret_cast<C*>(&sm.u[0][0]);
-    div_pass<0, C>(&sm.g[10][0], &sm.g[10][0], l, swz, A.tc.D, A.jac[0]);
-    div_pass<1, C>(&sm.g[0][0], divy, l, swz, A.tc.D, A.jac[1]);
-    div_pass<2, C>(&sm.g[5][0], &sm.g[5][0], l, swz, A.tc.D, A.jac[2]);
+    div_pass<0, C>(&sm.g[10][0], &sm.g[10][0], l, swz, A.sc.d[0]);
+    div_pass<1, C>(&sm.g[0][0], divy, l, swz, A.sc.d[1]);
+    div_pass<2, C>(&sm.g[5][0], &sm.g[5][0], l, swz, A.sc.d[2]);
     __syncthreads();
 
     // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
