@@ -141,6 +141,43 @@ int od_set_launch_shape(od_ctx* ctx, int elems_per_block_a, int elems_per_block_
  * do not depend on it. */
 int od_set_pipeline_slabs(od_ctx* ctx, int slabs);
 
+/* ------------------------------------------------------------------------
+ * z-slab domain decomposition: a mesh split along z over several contexts
+ * (one per GPU, or several on one), exchanging one layer of halo per phase.
+ * No counterpart in the reference (its solver runs one GPU).
+ * ------------------------------------------------------------------------ */
+
+/* Context for the z-layers z0 .. z1-1 of the mesh `params` (0 <= z0 < z1 <=
+ * nz). It holds those layers plus a ghost layer below and above; its state
+ * (od_state_bytes, od_set_state / od_get_state and the device variants) is
+ * the owned layers only, 5 planes of nx*ny*64*(z1-z0) values. Element size
+ * and Jacobians are those of the whole mesh, z is periodic across the slabs.
+ * od_step, od_rhs, od_diagnostics and od_attach_closure are not available on
+ * it: it steps stage by stage with od_slab_stage and the halo calls below. */
+int od_create_slab(const od_params* params, int z0, int z1, od_ctx** out);
+
+/* Phase A (phase 0) or phase B (phase 1) of SSP-RK3 stage `stage` (0..2) on
+ * the owned layers, enqueued on the context's stream. One stage is:
+ *   exchange kind 0 (the stage's input state), phase A,
+ *   exchange kind 1 (the z-face records phase A wrote), phase B.
+ * An exchange: od_slab_pack(dir 0) goes to the slab below, od_slab_pack(dir 1)
+ * to the slab above; the receiver calls od_slab_unpack with the same dir
+ * (dir 0: a message that travelled down, into the top ghost layer; dir 1: up,
+ * into the bottom ghost layer). With one slab, its own messages return to it.
+ * Results equal od_step on the whole mesh bit for bit. */
+int od_slab_stage(od_ctx* ctx, int stage, int phase, double dt);
+
+/* Bytes of one halo message: kind 0 = a z-layer of the state (5 x nx*ny*64
+ * state values), kind 1 = the layer's z-face records (dir 0: nx*ny*80, dir 1:
+ * nx*ny*64 compute-type values). 0 for invalid arguments. */
+size_t od_slab_halo_bytes(const od_ctx* ctx, int kind, int dir);
+
+/* Copy a halo message out of (pack) / into (unpack) the context: device
+ * buffers of od_slab_halo_bytes, enqueued on `stream` (null: the context's
+ * stream, ordered with its phases). */
+int od_slab_pack(od_ctx* ctx, int stage, int kind, int dir, void* d_dst, void* stream);
+int od_slab_unpack(od_ctx* ctx, int stage, int kind, int dir, const void* d_src, void* stream);
+
 /* Per-kernel timing: when enabled, every stage records CUDA events around its
  * phase-A and phase-B kernels; od_timing sums the recorded intervals since the
  * last reset (synchronizes the stream). */

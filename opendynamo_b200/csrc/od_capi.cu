@@ -148,6 +148,11 @@ struct od_ctx {
     long long n_stages = 0;
     od::StageHook hook = nullptr;   // learned closure between phase A and phase B
     void* hook_user = nullptr;
+    // z-slab of a decomposed mesh (od_create_slab): the local mesh holds the
+    // owned layers 1 .. nz-2 and a ghost layer below and above, which the
+    // caller fills between the phases (od_slab_unpack)
+    bool slab = false;
+    size_t buf_bytes = 0;     // one state buffer (state_bytes: the owned part the caller sees)
 };
 
 namespace {
@@ -161,6 +166,33 @@ int cuda_fail(od_ctx* c, cudaError_t e, const char* what) {
     return fail(c, OD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// jac = 2 / (L / n) in the compute type (rk.cu:93-95), from the mesh p
+void set_jac(od_ctx* c, const od_params* p) {
+    const double L3[3] = {p->lx, p->ly, p->lz};
+    const int n3[3] = {p->nx, p->ny, p->nz};
+    for (int d = 0; d < 3; ++d) {
+        if (c->fns.c_double)
+            c->jac[d] = 2.0 / (L3[d] / (double)n3[d]);
+        else
+            c->jac[d] = (double)(2.0f / ((float)L3[d] / (float)n3[d]));
+    }
+}
+
+// The caller-visible state of a context: all of U0, or for a slab its owned
+// layers (5 planes of nx*ny*64 points per owned layer, var-major).
+// to_ctx: other -> U0, else U0 -> other; kind: the copy direction.
+cudaError_t copy_state(od_ctx* c, void* other, bool to_ctx, cudaMemcpyKind kind) {
+    if (!c->slab) {
+        return to_ctx ? cudaMemcpyAsync(c->U[0], other, c->state_bytes, kind, c->stream)
+                      : cudaMemcpyAsync(other, c->U[0], c->state_bytes, kind, c->stream);
+    }
+    const size_t layer = (size_t)c->p.nx * c->p.ny * 64 * c->elem_size;
+    const size_t owned = c->state_bytes / 5, plane = c->buf_bytes / 5;
+    char* u = (char*)c->U[0] + layer;
+    return to_ctx ? cudaMemcpy2DAsync(u, plane, other, owned, owned, 5, kind, c->stream)
+                  : cudaMemcpy2DAsync(other, owned, u, plane, owned, 5, kind, c->stream);
+}
+
 int set_device(od_ctx* c) {
     cudaError_t e = cudaSetDevice(c->p.device);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
@@ -168,7 +200,9 @@ int set_device(od_ctx* c) {
 }
 
 // One stage: phase A (+ phase B) with the given buffers and RK coefficients.
-int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, double ra, double rb, double rc) {
+// The launch description of one stage on the context's buffers.
+od::StageLaunch make_launch(od_ctx* c, const void* u_in, const void* u0, void* u_out, double ra, double rb,
+                            double rc) {
     od::StageLaunch L{};
     L.u_in = u_in;
     L.u0 = u0;
@@ -193,6 +227,11 @@ int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, doub
     L.flux = c->p.flux;
     L.epb_a = c->epb_a;
     L.epb_b = c->epb_b;
+    return L;
+}
+
+int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, double ra, double rb, double rc) {
+    od::StageLaunch L = make_launch(c, u_in, u0, u_out, ra, rb, rc);
     cudaEvent_t tev[3] = {nullptr, nullptr, nullptr};
     if (c->timing) {
         while (c->events.size() < c->ev_used + 3) {
@@ -277,6 +316,25 @@ int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, doub
     return OD_OK;
 }
 
+// Buffers and coefficients of SSP-RK3 stage k (0..2): U0 -> U1, (U0, U1) ->
+// U2, (U0, U2) -> U0, coefficients evaluated in the state-arithmetic type
+// (solver.rs:256, 275-316).
+struct RkStage {
+    const void* u_in;
+    const void* u0;
+    void* u_out;
+    double ra, rb, rc;
+};
+
+RkStage rk_stage(od_ctx* c, int k, double dt) {
+    const bool pd = c->fns.p_double;
+    const double dtp = in_type(pd, dt);
+    if (k == 0) return {c->U[0], nullptr, c->U[1], 0.0, 1.0, dtp};
+    if (k == 1) return {c->U[1], c->U[0], c->U[2], 0.75, 0.25, in_type(pd, in_type(pd, 0.25) * dtp)};
+    return {c->U[2], c->U[0], c->U[0], in_type(pd, 1.0 / 3.0), in_type(pd, 2.0 / 3.0),
+            in_type(pd, in_type(pd, 2.0 / 3.0) * dtp)};
+}
+
 }  // namespace
 
 extern "C" {
@@ -346,15 +404,8 @@ int od_create(const od_params* p, od_ctx** out) {
     }
     if (c->fns.c_double && (p->ref_compat & OD_COMPAT_Y_SLICE_F32)) c->round_flags |= od::kRefYSlice;
     c->tab = build_tables();
-    // jac = 2 / (L / n) in the compute type (rk.cu:93-95)
-    const double L3[3] = {p->lx, p->ly, p->lz};
-    const int n3[3] = {p->nx, p->ny, p->nz};
-    for (int d = 0; d < 3; ++d) {
-        if (c->fns.c_double)
-            c->jac[d] = 2.0 / (L3[d] / (double)n3[d]);
-        else
-            c->jac[d] = (double)(2.0f / ((float)L3[d] / (float)n3[d]));
-    }
+    c->buf_bytes = c->state_bytes;
+    set_jac(c, p);
     int rc = set_device(c);
     if (rc) {
         *out = c;
@@ -384,7 +435,7 @@ int od_create(const od_params* p, od_ctx** out) {
         return cuda_fail(c, e, "kernel attributes");
     }
     for (int b = 0; b < 3; ++b) {
-        e = cudaMalloc(&c->U[b], c->state_bytes);
+        e = cudaMalloc(&c->U[b], c->buf_bytes);
         if (e != cudaSuccess) {
             *out = c;
             return cuda_fail(c, e, "cudaMalloc state");
@@ -393,7 +444,7 @@ int od_create(const od_params* p, od_ctx** out) {
     // An f32 state is rounded once per stage: the RK combination happens in
     // phase B, phase A hands over the unrounded RHS.
     if (!c->fns.s_double) {
-        e = cudaMalloc(&c->rhs, c->state_bytes);
+        e = cudaMalloc(&c->rhs, c->buf_bytes);
         if (e != cudaSuccess) {
             *out = c;
             return cuda_fail(c, e, "cudaMalloc RHS buffer");
@@ -437,7 +488,7 @@ int od_set_state(od_ctx* c, const void* host, size_t bytes) {
     if (!c || !host) return OD_ERR_ARG;
     if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
     if (int rc = set_device(c)) return rc;
-    cudaError_t e = cudaMemcpyAsync(c->U[0], host, bytes, cudaMemcpyHostToDevice, c->stream);
+    cudaError_t e = copy_state(c, const_cast<void*>(host), true, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "state upload");
     c->have_state = true;
@@ -449,7 +500,7 @@ int od_get_state(od_ctx* c, void* host, size_t bytes) {
     if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
     if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
     if (int rc = set_device(c)) return rc;
-    cudaError_t e = cudaMemcpyAsync(host, c->U[0], bytes, cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = copy_state(c, host, false, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "state download");
     return OD_OK;
@@ -459,7 +510,7 @@ int od_set_state_device(od_ctx* c, const void* dptr, size_t bytes) {
     if (!c || !dptr) return OD_ERR_ARG;
     if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
     if (int rc = set_device(c)) return rc;
-    cudaError_t e = cudaMemcpyAsync(c->U[0], dptr, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaError_t e = copy_state(c, const_cast<void*>(dptr), true, cudaMemcpyDeviceToDevice);
     if (e != cudaSuccess) return cuda_fail(c, e, "state copy");
     c->have_state = true;
     return OD_OK;
@@ -470,7 +521,7 @@ int od_get_state_device(od_ctx* c, void* dptr, size_t bytes) {
     if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
     if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
     if (int rc = set_device(c)) return rc;
-    cudaError_t e = cudaMemcpyAsync(dptr, c->U[0], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaError_t e = copy_state(c, dptr, false, cudaMemcpyDeviceToDevice);
     if (e != cudaSuccess) return cuda_fail(c, e, "state copy");
     return OD_OK;
 }
@@ -478,25 +529,125 @@ int od_get_state_device(od_ctx* c, void* dptr, size_t bytes) {
 int od_step(od_ctx* c, int n_steps, double dt) {
     if (!c || n_steps < 0) return OD_ERR_ARG;
     if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    if (c->slab) return fail(c, OD_ERR_STATE, "a slab context steps through od_slab_stage");
     if (int rc = set_device(c)) return rc;
-    // RK coefficients evaluated in the state-arithmetic type (solver.rs:256, 275-316)
-    const bool pd = c->fns.p_double;
-    const double dtp = in_type(pd, dt);
-    const double c1 = dtp;
-    const double c2 = in_type(pd, in_type(pd, 0.25) * dtp);
-    const double c3 = in_type(pd, in_type(pd, 2.0 / 3.0) * dtp);
-    const double a2 = 0.75, b2 = 0.25;
-    const double a3 = in_type(pd, 1.0 / 3.0), b3 = in_type(pd, 2.0 / 3.0);
-    for (int s = 0; s < n_steps; ++s) {
-        if (int rc = enqueue_stage(c, c->U[0], nullptr, c->U[1], 0.0, 1.0, c1)) return rc;
-        if (int rc = enqueue_stage(c, c->U[1], c->U[0], c->U[2], a2, b2, c2)) return rc;
-        if (int rc = enqueue_stage(c, c->U[2], c->U[0], c->U[0], a3, b3, c3)) return rc;
+    for (int s = 0; s < n_steps; ++s)
+        for (int k = 0; k < 3; ++k) {
+            const RkStage r = rk_stage(c, k, dt);
+            if (int rc = enqueue_stage(c, r.u_in, r.u0, r.u_out, r.ra, r.rb, r.rc)) return rc;
+        }
+    return OD_OK;
+}
+
+// ---- z-slab decomposition
+
+int od_create_slab(const od_params* g, int z0, int z1, od_ctx** out) {
+    if (!g || !out) return OD_ERR_ARG;
+    *out = nullptr;
+    if (z0 < 0 || z1 <= z0 || z1 > g->nz) return OD_ERR_ARG;
+    od_params p = *g;
+    p.nz = z1 - z0 + 2;   // owned layers + a ghost layer below and above
+    if (int rc = od_create(&p, out)) return rc;
+    od_ctx* c = *out;
+    set_jac(c, g);        // element size of the whole mesh
+    c->slab = true;
+    c->state_bytes = (size_t)p.nx * p.ny * (size_t)(z1 - z0) * 64 * 5 * c->elem_size;
+    return OD_OK;
+}
+
+int od_slab_stage(od_ctx* c, int stage, int phase, double dt) {
+    if (!c) return OD_ERR_ARG;
+    if (!c->slab) return fail(c, OD_ERR_STATE, "not a slab context (od_create_slab)");
+    if (stage < 0 || stage > 2 || (phase != 0 && phase != 1))
+        return fail(c, OD_ERR_ARG, "stage must be 0, 1 or 2 and phase 0 (A) or 1 (B)");
+    if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    if (int rc = set_device(c)) return rc;
+    const RkStage r = rk_stage(c, stage, dt);
+    od::StageLaunch L = make_launch(c, r.u_in, r.u0, r.u_out, r.ra, r.rb, r.rc);
+    const long long nxy = (long long)c->p.nx * c->p.ny;
+    L.e0 = nxy;               // the owned layers only
+    L.e1 = c->nelem - nxy;
+    L.phases = phase == 0 ? 1 : 2;
+    cudaError_t e = c->fns.launch(L, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, phase == 0 ? "slab phase A" : "slab phase B");
+    return OD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One halo message inside a slab context: `rows` rows of `width` bytes,
+// `pitch` bytes apart, starting at p. kind 0: the five planes of z-layer
+// `layer` of RK stage `stage`'s input state; kind 1: the z-face records of
+// the layer's elements — minus-face records F_I - Fv/2 (fi) or the plus-face
+// viscous fluxes (fv), direction 2 of [elem][dir 3][var][16].
+struct HaloBlock {
+    char* p;
+    size_t width, pitch, rows;
+};
+
+HaloBlock halo_block(od_ctx* c, int stage, int kind, int layer, bool fi) {
+    const size_t nxy = (size_t)c->p.nx * c->p.ny;
+    if (kind == 0) {
+        const size_t w = nxy * 64 * c->elem_size;
+        return {(char*)c->U[stage] + (size_t)layer * w, w, c->buf_bytes / 5, 5};
     }
+    const size_t cw = c->fns.c_double ? 8 : 4;
+    const size_t e0 = (size_t)layer * nxy;
+    if (fi) {
+        char* base = (char*)c->fv + (size_t)c->nelem * od::kFvWords * cw;
+        return {base + ((e0 * 3 + 2) * 80) * cw, 80 * cw, 240 * cw, nxy};
+    }
+    return {(char*)c->fv + ((e0 * 3 + 2) * 64) * cw, 64 * cw, 192 * cw, nxy};
+}
+
+int halo_args(od_ctx* c, int stage, int kind, int dir) {
+    if (!c) return OD_ERR_ARG;
+    if (!c->slab) return fail(c, OD_ERR_STATE, "not a slab context (od_create_slab)");
+    if (stage < 0 || stage > 2 || kind < 0 || kind > 1 || dir < 0 || dir > 1)
+        return fail(c, OD_ERR_ARG, "stage 0..2, kind 0 (state) or 1 (face records), dir 0 (down) or 1 (up)");
+    return set_device(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t od_slab_halo_bytes(const od_ctx* c, int kind, int dir) {
+    if (!c || !c->slab || kind < 0 || kind > 1 || dir < 0 || dir > 1) return 0;
+    const size_t nxy = (size_t)c->p.nx * c->p.ny;
+    if (kind == 0) return 5 * nxy * 64 * c->elem_size;
+    return nxy * (dir == 0 ? 80 : 64) * (c->fns.c_double ? 8 : 4);
+}
+
+int od_slab_pack(od_ctx* c, int stage, int kind, int dir, void* d_dst, void* stream) {
+    if (int rc = halo_args(c, stage, kind, dir)) return rc;
+    if (!d_dst) return OD_ERR_ARG;
+    // down: the lowest owned layer (its minus-face records); up: the highest (plus-face viscous fluxes)
+    const int layer = dir == 0 ? 1 : c->p.nz - 2;
+    const HaloBlock b = halo_block(c, stage, kind, layer, dir == 0);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    cudaError_t e = cudaMemcpy2DAsync(d_dst, b.width, b.p, b.pitch, b.width, b.rows, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(c, e, "slab halo pack");
+    return OD_OK;
+}
+
+int od_slab_unpack(od_ctx* c, int stage, int kind, int dir, const void* d_src, void* stream) {
+    if (int rc = halo_args(c, stage, kind, dir)) return rc;
+    if (!d_src) return OD_ERR_ARG;
+    // a message that travelled down fills the top ghost layer, one that travelled up the bottom one
+    const int layer = dir == 0 ? c->p.nz - 1 : 0;
+    const HaloBlock b = halo_block(c, stage, kind, layer, dir == 0);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    cudaError_t e = cudaMemcpy2DAsync(b.p, b.pitch, d_src, b.width, b.width, b.rows, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(c, e, "slab halo unpack");
     return OD_OK;
 }
 
 int od_rhs(od_ctx* c, void* d_out, size_t bytes) {
     if (!c || !d_out) return OD_ERR_ARG;
+    if (c->slab) return fail(c, OD_ERR_STATE, "not available on a slab context");
     if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "RHS size does not match the mesh");
     if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
     if (d_out == c->U[0] || (c->rhs && d_out == c->rhs))
@@ -507,6 +658,7 @@ int od_rhs(od_ctx* c, void* d_out, size_t bytes) {
 
 int od_diagnostics(od_ctx* c, double* vol6, double* prof, size_t prof_len) {
     if (!c || !vol6) return OD_ERR_ARG;
+    if (c->slab) return fail(c, OD_ERR_STATE, "not available on a slab context");
     if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
     const size_t nprof = (size_t)c->p.ny * 4 * 8;
     if (prof && prof_len < nprof) return fail(c, OD_ERR_SIZE, "profile buffer smaller than ny*4*8");
@@ -533,6 +685,7 @@ int od_diagnostics(od_ctx* c, double* vol6, double* prof, size_t prof_len) {
 
 int od_attach_closure(od_ctx* c, od_mlp* m) {
     if (!c) return OD_ERR_ARG;
+    if (c->slab && m) return fail(c, OD_ERR_STATE, "not available on a slab context");
     if (!m) {
         c->hook = nullptr;
         c->hook_user = nullptr;
