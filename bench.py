@@ -407,6 +407,61 @@ def run_closure_step(args, world, rank, local):
             "closure_gdof_stage_s": round(npts * 3 / (out["closure"] / 1e3) / 1e9, 3)}
 
 
+def run_slabs_form(args, world, rank, local):
+    """z-slab decomposition of the 48^3 channel on this GPU: the mesh in
+    --slabs slabs (each its own context and stream, halos exchanged between
+    the phases of every stage, stream-ordered), against the same mesh in one
+    context; the final states must agree bit for bit. CUDA events around the
+    step loop."""
+    if rank != 0:
+        return None
+    import torch
+    from opendynamo_b200 import slabs as SL
+    from opendynamo_b200.solver import Solver, make_params
+    torch.cuda.set_device(local)
+    w = WORKLOAD
+    u = build_state(np.float32)
+    dt = float(np.float32(w["dt"]))
+    steps = args.form_steps or RK_PER_STEP
+    p = make_params(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"], w["lz"], w["flux"], w["y_wall"], w["prec"],
+                    device=local)
+    npts = w["nx"] * w["ny"] * w["nz"] * 64
+
+    def timed(obj, step, sync):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        step(args.warmup)
+        sync()
+        torch.cuda.synchronize()
+        ev0.record()
+        torch.cuda.synchronize()
+        step(steps)
+        sync()
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1)
+
+    with Solver(p) as s:
+        s.set_state(u)
+        ms_one = timed(s, lambda n: s.step(n, dt), s.sync)
+        ref = s.get_state()
+    d = SL.LocalSlabs(p, args.slabs)
+    try:
+        d.set_state(u)
+        ms_sl = timed(d, lambda n: d.step(n, dt), d.sync)
+        got = d.get_state()
+        halo = sum(d.slabs[0].halo_bytes(k, dr) for k in SL.KINDS for dr in (SL.DOWN, SL.UP))
+    finally:
+        d.close()
+    rate = lambda ms: npts * 3 * steps / (ms / 1e3) / 1e9
+    return {"metric": f"Gdof*stage/s, 48^3 channel in {args.slabs} z-slabs on one GPU", "value": round(rate(ms_sl), 3),
+            "unit": "Gdof*stage/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (channel IC generator, seed 42)",
+            "config": {"workload": "channel 48^3, SLAU2, y walls, f32", "form": "slabs", "slabs": args.slabs,
+                       "halo_bytes_per_slab_and_stage": int(halo)},
+            "whole_mesh_value": round(rate(ms_one), 3), "bit_identical": bool(np.array_equal(got, ref)),
+            "ms_per_step": round(ms_sl / steps, 4), "whole_ms_per_step": round(ms_one / steps, 4)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -414,7 +469,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="plain", choices=["plain", "precision", "ensemble", "closure", "closure-step"],
+    ap.add_argument("--form", default="plain",
+                    choices=["plain", "precision", "ensemble", "closure", "closure-step", "slabs"],
                     help="plain: the headline 48^3 bench; precision: the precision-form study")
     ap.add_argument("--mesh", type=int, default=0, help="elements per axis of a --form run (0 = its default)")
     ap.add_argument("--form-steps", type=int, default=0, help="RK3 steps of a --form run (0 = its default)")
@@ -423,6 +479,7 @@ def main():
     ap.add_argument("--snaps", type=int, default=0, help="closure: snapshots per training seed (0 = 125)")
     ap.add_argument("--epochs", type=int, default=0, help="closure: training epochs (0 = 8)")
     ap.add_argument("--save-weights", default="", help="closure: write the trained network (.npz)")
+    ap.add_argument("--slabs", type=int, default=4, help="slabs: number of z-slabs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -437,6 +494,8 @@ def main():
         out = run_closure_form(args, world, rank, local)
     elif args.form == "closure-step":
         out = run_closure_step(args, world, rank, local)
+    elif args.form == "slabs":
+        out = run_slabs_form(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if out is not None and rank == 0:

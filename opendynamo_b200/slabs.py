@@ -157,6 +157,10 @@ class LocalSlabs:
         # message buffers: [slab][kind][direction]
         self._buf = [[[torch.empty(s.halo_bytes(k, d), dtype=torch.uint8, device=s.torch_device)
                        for d in (DOWN, UP)] for k in KINDS] for s in self.slabs]
+        # ordering between the slabs' streams: nothing waits on the host
+        self._streams = [torch.cuda.ExternalStream(s.stream, device=s.torch_device) for s in self.slabs]
+        self._packed = [[torch.cuda.Event() for _ in KINDS] for _ in self.slabs]
+        self._read = [[None for _ in KINDS] for _ in self.slabs]   # neighbours done reading my buffers
 
     def close(self) -> None:
         for s in self.slabs:
@@ -171,22 +175,34 @@ class LocalSlabs:
         return np.concatenate(parts, axis=1).reshape(-1)
 
     def _exchange(self, stage: int, kind: int) -> None:
+        """Stream-ordered: a slab packs once its neighbours have read its
+        previous messages of this kind, unpacks once they have packed."""
+        import torch
         n = len(self.slabs)
-        for s in self.slabs:
-            s.sync()   # the previous exchange's reads of these buffers are done
-        for s, b in zip(self.slabs, self._buf):
+        for r, (s, b, st) in enumerate(zip(self.slabs, self._buf, self._streams)):
+            for ev in self._read[r][kind] or ():
+                st.wait_event(ev)
             s.pack(stage, kind, DOWN, b[kind][DOWN])
             s.pack(stage, kind, UP, b[kind][UP])
-        for s in self.slabs:
-            s.sync()
-        for r, s in enumerate(self.slabs):
-            above, below = self._buf[(r + 1) % n][kind][DOWN], self._buf[(r - 1) % n][kind][UP]
+            self._packed[r][kind].record(st)
+        done = []
+        for r, (s, st) in enumerate(zip(self.slabs, self._streams)):
+            a, b = (r + 1) % n, (r - 1) % n
+            st.wait_event(self._packed[a][kind])
+            st.wait_event(self._packed[b][kind])
+            above, below = self._buf[a][kind][DOWN], self._buf[b][kind][UP]
             if above.device != s.torch_device or below.device != s.torch_device:
-                import torch
-                above, below = above.to(s.torch_device), below.to(s.torch_device)
-                torch.cuda.synchronize(s.torch_device)
+                with torch.cuda.stream(st):
+                    above = above.to(s.torch_device, non_blocking=True)
+                    below = below.to(s.torch_device, non_blocking=True)
             s.unpack(stage, kind, DOWN, above)
             s.unpack(stage, kind, UP, below)
+            ev = torch.cuda.Event()
+            ev.record(st)
+            done.append(ev)
+        for r in range(n):
+            # my buffers are read by the slabs above and below
+            self._read[r][kind] = (done[(r + 1) % n], done[(r - 1) % n])
 
     def step(self, n_steps: int, dt: float) -> None:
         _step_slabs(self.slabs, self._exchange, n_steps, dt)
