@@ -101,6 +101,17 @@ int od_set_state(od_ctx* ctx, const void* host, size_t bytes);
  * Replaces: the dump copy io_stream.memcpy_dtoh (src/solver.rs:757-759). */
 int od_get_state(od_ctx* ctx, void* host, size_t bytes);
 
+/* Asynchronous download: the state as of this point of the context's stream
+ * goes to `host` (pinned for a truly asynchronous copy) on `stream`; the call
+ * returns at once and later od_step calls may run meanwhile — the copy reads
+ * a device snapshot taken on the context's stream. The data is in `host` once
+ * `stream` has passed this point (synchronise it or an event on it). A null
+ * stream makes it od_get_state. One snapshot per context: a second call
+ * waits, on the device, for the first download to finish.
+ * Replaces: the dump copy on the IO stream with its event hand-off
+ * (src/solver.rs:161-175, 745-759). */
+int od_get_state_async(od_ctx* ctx, void* host, size_t bytes, void* stream);
+
 /* Same as above from / to device memory (stream-ordered, no host sync). */
 int od_set_state_device(od_ctx* ctx, const void* dptr, size_t bytes);
 int od_get_state_device(od_ctx* ctx, void* dptr, size_t bytes);

@@ -153,6 +153,9 @@ struct od_ctx {
     // caller fills between the phases (od_slab_unpack)
     bool slab = false;
     size_t buf_bytes = 0;     // one state buffer (state_bytes: the owned part the caller sees)
+    // od_get_state_async: device snapshot of the state and its two events
+    void* snap = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_copied = nullptr;
 };
 
 namespace {
@@ -477,6 +480,9 @@ void od_destroy(od_ctx* c) {
         if (c->U[b]) cudaFree(c->U[b]);
     if (c->fv) cudaFree(c->fv);
     if (c->rhs) cudaFree(c->rhs);
+    if (c->snap) cudaFree(c->snap);
+    if (c->ev_snap) cudaEventDestroy(c->ev_snap);
+    if (c->ev_copied) cudaEventDestroy(c->ev_copied);
     if (c->stream_b) cudaStreamDestroy(c->stream_b);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -503,6 +509,34 @@ int od_get_state(od_ctx* c, void* host, size_t bytes) {
     cudaError_t e = copy_state(c, host, false, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "state download");
+    return OD_OK;
+}
+
+int od_get_state_async(od_ctx* c, void* host, size_t bytes, void* stream) {
+    if (!stream) return od_get_state(c, host, bytes);
+    if (!c || !host) return OD_ERR_ARG;
+    if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
+    if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+    if (int rc = set_device(c)) return rc;
+    cudaError_t e = cudaSuccess;
+    if (!c->snap) {
+        e = cudaMalloc(&c->snap, c->state_bytes);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_snap, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_copied, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "state snapshot buffer");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    // the compute stream: wait until the previous download has read the
+    // snapshot, take a new one (a device copy), and carry on
+    e = cudaStreamWaitEvent(c->stream, c->ev_copied, 0);
+    if (e == cudaSuccess) e = copy_state(c, c->snap, false, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_snap, c->stream);
+    // the caller's stream: download the snapshot
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->ev_snap, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, c->snap, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_copied, s);
+    if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous state download");
     return OD_OK;
 }
 
