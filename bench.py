@@ -129,8 +129,9 @@ def build_state(dtype=np.float32):
 
 
 def cpu_baseline(u: np.ndarray) -> dict:
-    """The project's multithreaded FP64 oracle on this host's cores: one RK3
-    step of the 48^3 channel (a bounded sample of the workload)."""
+    """The project's multithreaded FP64 oracle on this host's cores: SSP-RK3
+    steps of the 48^3 channel until about 12 s of CPU work (a bounded sample
+    of the workload; one step first, then as many more as fit)."""
     import oracle
     w = WORKLOAD
     cores = os.cpu_count() or 1
@@ -139,11 +140,16 @@ def cpu_baseline(u: np.ndarray) -> dict:
     u64 = u.astype(np.float64)
     oracle.lib()
     t0 = time.perf_counter()
-    oracle.run(p, u64, 1, w["dt"])
+    u64 = oracle.run(p, u64, 1, w["dt"])
+    first = time.perf_counter() - t0
+    more = max(0, min(15, int(12.0 / max(first, 1e-3)) - 1))
+    if more:
+        oracle.run(p, u64, more, w["dt"])
     sec = time.perf_counter() - t0
+    steps = 1 + more
     npts = w["nx"] * w["ny"] * w["nz"] * 64
-    return {"value": npts * 3 / sec / 1e9, "unit": "Gdof*stage/s", "cores": cores, "kind": "port",
-            "sample": f"1 SSP-RK3 step (3 stages) of the 48^3 channel in FP64, {sec:.2f} s"}
+    return {"value": npts * 3 * steps / sec / 1e9, "unit": "Gdof*stage/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} SSP-RK3 steps ({3 * steps} stages) of the 48^3 channel in FP64, {sec:.2f} s"}
 
 
 def run_ours(args, world, rank, local):
