@@ -382,7 +382,7 @@ int od_create(const od_params* p, od_ctx** out) {
         (p->viscosity_model != OD_VISC_SUTHERLAND || !(p->t_ref > 0) || !(p->s_suth >= 0)))
         return OD_ERR_ARG;
     long long nelem = (long long)p->nx * p->ny * p->nz;
-    if (nelem * 64 * 5 >= (1LL << 40)) return OD_ERR_ARG;
+    if (nelem >= (1LL << 31)) return OD_ERR_ARG;   // element indices are 32-bit in the kernels
     od_ctx* c = new od_ctx();
     c->p = *p;
     c->nelem = nelem;

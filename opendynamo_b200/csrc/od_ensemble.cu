@@ -328,6 +328,7 @@ int build_stage_params(od_ensemble* E) {
             A.m.nz = x.nz;
             A.m.y_wall = x.y_wall;
             A.m.nelem = E->nelem[b];
+            od::mesh_set_div(A.m);
             A.m.npts = E->nelem[b] * NE;
             const double L3[3] = {x.lx, x.ly, x.lz};
             const int n3[3] = {x.nx, x.ny, x.nz};

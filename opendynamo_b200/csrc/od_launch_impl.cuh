@@ -78,6 +78,7 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.m.nz = L.nz;
     A.m.y_wall = L.y_wall;
     A.m.nelem = L.nelem;
+    mesh_set_div(A.m);
     A.m.npts = L.nelem * NE;
     A.tp = cast_tab<P>(L.tab);
     A.tc = cast_tab<C>(L.tab);

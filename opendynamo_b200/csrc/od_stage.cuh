@@ -91,10 +91,52 @@ __host__ ScaledTab<T> scale_tab(const TabT& t, const T* jac) {
     return r;
 }
 
+// Division of a 32-bit unsigned value by a divisor fixed for the launch: a
+// multiply-high and two shifts instead of the integer division sequence
+// (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, section 4): with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, n / d = (t + ((n - t) >> min(l, 1))) >>
+// max(l - 1, 0) where t = mulhi(m, n), for every n and d in [1, 2^32).
+struct FastDiv {
+    unsigned m, s1, s2;
+};
+
+__host__ inline FastDiv make_fastdiv(unsigned d) {
+    unsigned l = 0;
+    while (l < 32 && (1ull << l) < d) ++l;
+    FastDiv f;
+    f.m = (unsigned)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+    f.s1 = l < 1 ? l : 1;
+    f.s2 = l > 0 ? l - 1 : 0;
+    return f;
+}
+
+__device__ __forceinline__ unsigned fast_div(unsigned n, const FastDiv& f) {
+    const unsigned t = __umulhi(f.m, n);
+    return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
+// Element indices are below 2^31 (od_create rejects larger meshes).
 struct Mesh {
     int nx, ny, nz, y_wall;
     long long nelem, npts;
+    FastDiv fx, fy;   // division by nx and by ny
 };
+
+__host__ inline void mesh_set_div(Mesh& m) {
+    m.fx = make_fastdiv((unsigned)m.nx);
+    m.fy = make_fastdiv((unsigned)m.ny);
+}
+
+// (ex, ey, ez) of element e = ex + nx (ey + ny ez)
+__device__ __forceinline__ void elem_coords(const Mesh& m, long long e, int& ex, int& ey, int& ez) {
+    const unsigned u = (unsigned)e;
+    const unsigned q = fast_div(u, m.fx);
+    const unsigned q2 = fast_div(q, m.fy);
+    ex = (int)(u - q * (unsigned)m.nx);
+    ey = (int)(q - q2 * (unsigned)m.ny);
+    ez = (int)q2;
+}
 
 // point index inside an element: i + 4 j + 16 k
 __device__ __forceinline__ constexpr int pid(int i, int j, int k) { return i + NP * j + NF * k; }
@@ -149,7 +191,7 @@ __device__ __forceinline__ long long neighbour(const Mesh& m, int ex, int ey, in
         c2 += side ? 1 : -1;
         c2 = c2 < 0 ? c2 + m.nz : (c2 >= m.nz ? c2 - m.nz : c2);
     }
-    return (long long)c0 + (long long)m.nx * ((long long)c1 + (long long)m.ny * c2);
+    return (long long)(c0 + m.nx * (c1 + m.ny * c2));
 }
 
 // ---- 4-wide loads / stores (16-byte aligned for float, 32-byte for double)
@@ -581,9 +623,8 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     const bool live = e < A.e1;
     const long long ec = live ? e : 0;
     const Mesh& m = A.m;
-    const int ex = (int)(ec % m.nx);
-    const int ey = (int)((ec / m.nx) % m.ny);
-    const int ez = (int)(ec / ((long long)m.nx * m.ny));
+    int ex, ey, ez;
+    elem_coords(m, ec, ex, ey, ez);
     const long long nxm = neighbour(m, ex, ey, ez, 0, 0), nxp = neighbour(m, ex, ey, ez, 0, 1);
     const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
     const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
@@ -713,9 +754,8 @@ __device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
     const long long e = B.e0 + tile * EPB + threadIdx.x / LPE;
     const Mesh& m = B.m;
     if (e >= B.e1) return;
-    const int ex = (int)(e % m.nx);
-    const int ey = (int)((e / m.nx) % m.ny);
-    const int ez = (int)(e / ((long long)m.nx * m.ny));
+    int ex, ey, ez;
+    elem_coords(m, e, ex, ey, ez);
     const int lj = l & 3, lk = l >> 2;
     const long long nxm = neighbour(m, ex, ey, ez, 0, 0), nxp = neighbour(m, ex, ey, ez, 0, 1);
     const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
