@@ -17,7 +17,7 @@ import oracle
 from helpers import assert_f32_parity, channel_trip, random_smooth, rel_l2, tgv
 from opendynamo_b200.solver import Solver, make_params
 
-MESHES = [(2, 3, 4), (3, 3, 3), (4, 1, 5)]
+MESHES = [(2, 3, 4), (3, 3, 3), (4, 1, 5), (1, 1, 1), (1, 3, 2), (7, 5, 3)]
 BOX = (2 * math.pi, 2.0, math.pi)
 RHS_TOL = {"f64": 1e-11, "f32": 5e-5}
 
