@@ -356,36 +356,61 @@ __device__ __forceinline__ void plus_face(const P* own, bool wall, C* j) {
     for (int v = 0; v < NV; ++v) j[v] = -fe[v];
 }
 
-// load / store the 4 samples of line l in direction D of a swizzled row
+// Swizzled row offsets of the three lines of thread l, computed once per
+// tile: x-line start, the four y-line points and the two z-line bases
+// (points mm < 2 and mm >= 2, + 16 mm).
+struct LineIdx {
+    int x;
+    int y[4];
+    int z[2];
+};
+
+__device__ __forceinline__ LineIdx line_idx(int l, int swz) {
+    LineIdx li;
+    li.x = sw(4 * l, swz);
+#pragma unroll
+    for (int mm = 0; mm < 4; ++mm) li.y[mm] = sw(line_pt<1>(l, mm), swz);
+    li.z[0] = sw(line_pt<2>(l, 0), swz);
+    li.z[1] = sw(line_pt<2>(l, 2), swz) - 32;
+    return li;
+}
+
+template <int D>
+__device__ __forceinline__ int line_off(const LineIdx& li, int mm) {
+    if constexpr (D == 1) return li.y[mm];
+    else return li.z[mm >> 1] + 16 * mm;
+}
+
+// load / store the 4 samples of the thread's direction-D line of a swizzled row
 template <int D, class T>
-__device__ __forceinline__ void row_line_load(const T* row, int l, int swz, T* w) {
+__device__ __forceinline__ void row_line_load(const T* row, const LineIdx& li, T* w) {
     if constexpr (D == 0) {
-        ld4s(row + sw(4 * l, swz), w);
+        ld4s(row + li.x, w);
     } else {
 #pragma unroll
-        for (int mm = 0; mm < 4; ++mm) w[mm] = row[sw(line_pt<D>(l, mm), swz)];
+        for (int mm = 0; mm < 4; ++mm) w[mm] = row[line_off<D>(li, mm)];
     }
 }
 
 template <int D, class T>
-__device__ __forceinline__ void row_line_store(T* row, int l, int swz, const T* w) {
+__device__ __forceinline__ void row_line_store(T* row, const LineIdx& li, const T* w) {
     if constexpr (D == 0) {
-        st4s(row + sw(4 * l, swz), w);
+        st4s(row + li.x, w);
     } else {
 #pragma unroll
-        for (int mm = 0; mm < 4; ++mm) row[sw(line_pt<D>(l, mm), swz)] = w[mm];
+        for (int mm = 0; mm < 4; ++mm) row[line_off<D>(li, mm)] = w[mm];
     }
 }
 
 // P2-P4: one direction of the gradient / face-value pass for line l.
 template <class M, int FLUX, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
-__device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, int swz, const long long nb0,
+__device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, const LineIdx& li, const long long nb0,
                                           const long long nb1, P* oL, P* oR, C (&jx)[2][NV], C* fi) {
     using S = typename PA::S_t;
     const Mesh& m = A.m;
     P q[NV][4];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) row_line_load<D>(sm.u[v], l, swz, q[v]);
+    for (int v = 0; v < NV; ++v) row_line_load<D>(sm.u[v], li, q[v]);
     P nL[NV], nR[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -435,7 +460,7 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, i
             }
             gv[a] = gg;
         }
-        row_line_store<D>(sm.g[3 * v + D], l, swz, gv);
+        row_line_store<D>(sm.g[3 * v + D], li, gv);
     }
     // inviscid parts at the two faces of this line; F_I stays in registers
     // until the minus face's viscous flux is known (P5)
@@ -500,7 +525,7 @@ __device__ __forceinline__ C ref_y_slice(const C* w, const CC& c) {
 // flux at both faces of the line.
 template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, long long e, int l,
-                                               int swz, bool wall0, bool wall1, bool live, const P* tL,
+                                               const LineIdx& li, bool wall0, bool wall1, bool live, const P* tL,
                                                const P* tR, C (&jx)[2][NV], const C* fi) {
     if (wall0 && wall1) return;
     C gL[15], gR[15];
@@ -513,7 +538,7 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
             continue;
         }
         C w[4];
-        row_line_load<D>(sm.g[c], l, swz, w);
+        row_line_load<D>(sm.g[c], li, w);
         if (ref_y) {
             gL[c] = ref_y_slice(w, A.tc.eL);
             gR[c] = ref_y_slice(w, A.tc.eR);
@@ -530,7 +555,7 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
             qR[v] = tR[v];
         } else {
             P w[4];
-            row_line_load<D>(sm.u[v], l, swz, w);
+            row_line_load<D>(sm.u[v], li, w);
             trace4_lr(w, A.tp.eL, A.tp.eR, qL[v], qR[v]);
         }
     }
@@ -541,14 +566,14 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
 // P7: divergence of F_D along the line of thread l (Dm: the Jacobian-scaled
 // derivative of direction D).
 template <int D, class C, class DM>
-__device__ __forceinline__ void div_pass(const C* F, C* out, int l, int swz, const DM& Dm) {
+__device__ __forceinline__ void div_pass(const C* F, C* out, const LineIdx& li, const DM& Dm) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C w[4];
-        row_line_load<D>(F + v * NE, l, swz, w);
+        row_line_load<D>(F + v * NE, li, w);
         C r[4];
         deriv4(w, Dm, r);
-        row_line_store<D>(out + v * NE, l, swz, r);
+        row_line_store<D>(out + v * NE, li, r);
     }
 }
 
@@ -618,6 +643,7 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     const int l = threadIdx.x & (LPE - 1);
     const int es = threadIdx.x / LPE;
     const int swz = (es & 1) << 3;
+    const LineIdx li = line_idx(l, swz);
     SlotA<P, C>& sm = reinterpret_cast<SlotA<P, C>*>(smem_raw)[es];
     const long long e = A.e0 + tile * EPB + es;
     const bool live = e < A.e1;
@@ -647,15 +673,15 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     P tr[3][2][NV];   // own face values of this thread's lines (kept only for f32 state arithmetic)
     C jx[2][NV];      // this x-line's x-face corrections
     C fi[3][NV];      // interface fluxes at the minus faces of this thread's lines
-    line_pass<M, FLUX, 0>(A, sm, l, swz, nxm, nxp, tr[0][0], tr[0][1], jx, fi[0]);
-    line_pass<M, FLUX, 1>(A, sm, l, swz, nym, nyp, tr[1][0], tr[1][1], jx, fi[1]);
-    line_pass<M, FLUX, 2>(A, sm, l, swz, nzm, nzp, tr[2][0], tr[2][1], jx, fi[2]);
+    line_pass<M, FLUX, 0>(A, sm, l, li, nxm, nxp, tr[0][0], tr[0][1], jx, fi[0]);
+    line_pass<M, FLUX, 1>(A, sm, l, li, nym, nyp, tr[1][0], tr[1][1], jx, fi[1]);
+    line_pass<M, FLUX, 2>(A, sm, l, li, nzm, nzp, tr[2][0], tr[2][1], jx, fi[2]);
     __syncthreads();
 
     // ---- P5: viscous face fluxes of all six faces, face records
-    face_grad_pass<M, 0>(A, sm, ec, l, swz, false, false, live, tr[0][0], tr[0][1], jx, fi[0]);
-    face_grad_pass<M, 1>(A, sm, ec, l, swz, nym < 0, nyp < 0, live, tr[1][0], tr[1][1], jx, fi[1]);
-    face_grad_pass<M, 2>(A, sm, ec, l, swz, false, false, live, tr[2][0], tr[2][1], jx, fi[2]);
+    face_grad_pass<M, 0>(A, sm, ec, l, li, false, false, live, tr[0][0], tr[0][1], jx, fi[0]);
+    face_grad_pass<M, 1>(A, sm, ec, l, li, nym < 0, nyp < 0, live, tr[1][0], tr[1][1], jx, fi[1]);
+    face_grad_pass<M, 2>(A, sm, ec, l, li, false, false, live, tr[2][0], tr[2][1], jx, fi[2]);
     __syncthreads();
 
     // ---- P6: pointwise fluxes of the x-line's points (own points only; the
@@ -691,9 +717,9 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
 
     // ---- P7: divergences: x in place (rows 10-14), y -> state region, z in place (rows 5-9)
     C* divy = reinterpret_cast<C*>(&sm.u[0][0]);
-    div_pass<0, C>(&sm.g[10][0], &sm.g[10][0], l, swz, A.sc.d[0]);
-    div_pass<1, C>(&sm.g[0][0], divy, l, swz, A.sc.d[1]);
-    div_pass<2, C>(&sm.g[5][0], &sm.g[5][0], l, swz, A.sc.d[2]);
+    div_pass<0, C>(&sm.g[10][0], &sm.g[10][0], li, A.sc.d[0]);
+    div_pass<1, C>(&sm.g[0][0], divy, li, A.sc.d[1]);
+    div_pass<2, C>(&sm.g[5][0], &sm.g[5][0], li, A.sc.d[2]);
     __syncthreads();
 
     // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
