@@ -688,9 +688,6 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     // point order is rotated by k so the 16 lanes of an element hit distinct banks)
     {
         const int lk = l >> 2;
-        P qx[NV][4];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) ld4s(&sm.u[v][sw(4 * l, swz)], qx[v]);
 #pragma unroll 1
         for (int it = 0; it < 4; ++it) {
             const int i = (it + lk) & 3;
@@ -700,7 +697,7 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
             for (int c = 0; c < 15; ++c) g[c] = sm.g[c][p];
             P qp[NV];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) qp[v] = i == 0 ? qx[v][0] : i == 1 ? qx[v][1] : i == 2 ? qx[v][2] : qx[v][3];
+            for (int v = 0; v < NV; ++v) qp[v] = sm.u[v][p];
             C praw;
             FaceState<C> s = make_face_state<M, C, P>(qp, praw);
             C F[3][NV];
