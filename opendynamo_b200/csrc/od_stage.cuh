@@ -416,7 +416,7 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, c
     for (int v = 0; v < NV; ++v) {
         trace4_lr(q[v], A.tp.eL, A.tp.eR, oL[v], oR[v]);
         const P refl = (v > 0 && v < 4) ? (P)-1.0 : (P)1.0;
-        if (nb0 >= 0) {
+        if (D != 1 || nb0 >= 0) {   // only y can have walls: x and z neighbours always exist
             P w[4];
             const S* base = A.u_in + v * m.npts + nb0 * NE;
             if constexpr (D == 0) {
@@ -429,7 +429,7 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, c
         } else {
             nL[v] = oL[v] * refl;
         }
-        if (nb1 >= 0) {
+        if (D != 1 || nb1 >= 0) {
             P w[4];
             const S* base = A.u_in + v * m.npts + nb1 * NE;
             if constexpr (D == 0) {
@@ -465,8 +465,8 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, c
     // inviscid parts at the two faces of this line; F_I stays in registers
     // until the minus face's viscous flux is known (P5)
     C j0[NV], j1[NV];
-    minus_face<M, FLUX, D, P, C>(oL, nL, nb0 < 0, j0, fi, A.flux);
-    plus_face<M, D, P, C>(oR, nb1 < 0, j1);
+    minus_face<M, FLUX, D, P, C>(oL, nL, D == 1 && nb0 < 0, j0, fi, A.flux);
+    plus_face<M, D, P, C>(oR, D == 1 && nb1 < 0, j1);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         if constexpr (D == 0) {
