@@ -138,10 +138,12 @@ void* od_stream(od_ctx* ctx);
 int od_launches_per_step(const od_ctx* ctx);
 
 /* Launch shape: elements per thread block of the phase-A kernel (2 or 4;
- * 16 threads per element) and of the phase-B kernel (8 or 16). Default 4 / 8
- * (fastest measured on B200). The phase-B shape and the z-slab setting do not
- * change results; the two phase-A shapes are separate kernels and agree to
- * round-off (the compiler may contract a multiply-add differently). */
+ * 16 threads per element) and of phase B: 8 or 16 with a thread per x-line
+ * (all five variables), or 2 or 4 with a thread per x-line and variable (80
+ * threads per element). Default 4 / 2 (fastest measured on B200). The
+ * phase-B shape and the z-slab setting do not change results; the two
+ * phase-A shapes are separate kernels and agree to round-off (the compiler
+ * may contract a multiply-add differently). */
 int od_set_launch_shape(od_ctx* ctx, int elems_per_block_a, int elems_per_block_b);
 
 /* z-slab pipeline: each stage runs phase A slab by slab on the context's

@@ -138,9 +138,11 @@ struct od_ctx {
     double jac[3] = {0, 0, 0};
     int round_flags = 0;
     bool have_state = false;
-    // launch shape: 4 elements per phase-A block, 8 per phase-B block (B200,
-    // 48^3 f32: phase B 0.132 ms at 8 against 0.142 at 16; phase A 2 vs 4 equal)
-    int epb_a = 4, epb_b = 8;
+    // launch shape: 4 elements per phase-A block; phase B with a thread per
+    // (element, variable, x-line), 2 elements per block (B200, 48^3 f32: phase
+    // B 0.122 ms against 0.128 with a thread per x-line and 8 elements, 0.136
+    // with 16; phase A 2 vs 4 equal)
+    int epb_a = 4, epb_b = 2;
     std::string err;
     bool timing = false;
     std::vector<cudaEvent_t> events;
@@ -766,8 +768,9 @@ int od_set_launch_shape(od_ctx* c, int elems_per_block_a, int elems_per_block_b)
     if (!c) return OD_ERR_ARG;
     if (elems_per_block_a != 2 && elems_per_block_a != 4)
         return fail(c, OD_ERR_ARG, "phase-A elements per block must be 2 or 4");
-    if (elems_per_block_b != 8 && elems_per_block_b != 16)
-        return fail(c, OD_ERR_ARG, "phase-B elements per block must be 8 or 16");
+    if (elems_per_block_b != 2 && elems_per_block_b != 4 && elems_per_block_b != 8 && elems_per_block_b != 16)
+        return fail(c, OD_ERR_ARG, "phase-B elements per block must be 8 or 16 (a thread per x-line) or 2 or 4 "
+                                   "(a thread per x-line and variable)");
     c->epb_a = elems_per_block_a;
     c->epb_b = elems_per_block_b;
     return OD_OK;

@@ -61,6 +61,14 @@ cudaError_t launch_b(const StageBParams<S, P, C>& B, long long nelem, cudaStream
     return cudaGetLastError();
 }
 
+template <class S, class P, class C, int EPB>
+cudaError_t launch_b_split(const StageBParams<S, P, C>& B, long long nelem, cudaStream_t s) {
+    const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
+    if (grid == 0) return cudaSuccess;
+    stage_b_split_kernel<S, P, C, EPB><<<grid, LPE * NV * EPB, 0, s>>>(B);
+    return cudaGetLastError();
+}
+
 // fast math changes only f32 arithmetic: f64-compute combinations use one variant
 template <class C>
 constexpr bool has_fast_variant() { return sizeof(C) == 4; }
@@ -128,8 +136,12 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
         B.e1 = L.e1;
         if (L.epb_b == 8)
             err = launch_b<S, P, C, 8>(B, count, s);
-        else
+        else if (L.epb_b == 16)
             err = launch_b<S, P, C, 16>(B, count, s);
+        else if (L.epb_b == 2)
+            err = launch_b_split<S, P, C, 2>(B, count, s);
+        else
+            err = launch_b_split<S, P, C, 4>(B, count, s);
         if (err != cudaSuccess) return err;
         if (L.ev[2]) cudaEventRecord(L.ev[2], s);
     }

@@ -768,102 +768,147 @@ __device__ __forceinline__ T ldf(const T* p) {
 // One tile of phase B: EPB elements starting at B.e0 + tile * EPB. COH: the
 // face buffers and the RHS were written by this same launch (a persistent
 // kernel after its grid barrier), so they are read through the coherent path.
-template <int EPB, bool COH, class PB>
-__device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
-    using S = typename PB::S_t;
-    using P = typename PB::P_t;
-    using C = typename PB::C_t;
-    const int l = threadIdx.x & (LPE - 1);
-    const long long e = B.e0 + tile * EPB + threadIdx.x / LPE;
+// Per-element context of phase B: the element, its x-line and its neighbours.
+template <class C>
+struct BCtx {
+    long long e, nxm, nxp, nym, nyp, nzm, nzp;
+    int l, lj, lk;
+    C hx, hy, hz;
+};
+
+template <class PB, class C = typename PB::C_t>
+__device__ __forceinline__ BCtx<C> b_ctx(const PB& B, long long e, int l) {
+    BCtx<C> x;
     const Mesh& m = B.m;
-    if (e >= B.e1) return;
     int ex, ey, ez;
     elem_coords(m, e, ex, ey, ez);
-    const int lj = l & 3, lk = l >> 2;
-    const long long nxm = neighbour(m, ex, ey, ez, 0, 0), nxp = neighbour(m, ex, ey, ez, 0, 1);
-    const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
-    const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
-    const C hx = (C)0.5 * B.jac[0], hy = (C)0.5 * B.jac[1], hz = (C)0.5 * B.jac[2];
+    x.e = e;
+    x.l = l;
+    x.lj = l & 3;
+    x.lk = l >> 2;
+    x.nxm = neighbour(m, ex, ey, ez, 0, 0);
+    x.nxp = neighbour(m, ex, ey, ez, 0, 1);
+    x.nym = neighbour(m, ex, ey, ez, 1, 0);
+    x.nyp = neighbour(m, ex, ey, ez, 1, 1);
+    x.nzm = neighbour(m, ex, ey, ez, 2, 0);
+    x.nzp = neighbour(m, ex, ey, ez, 2, 1);
+    x.hx = (C)0.5 * B.jac[0];
+    x.hy = (C)0.5 * B.jac[1];
+    x.hz = (C)0.5 * B.jac[2];
+    return x;
+}
+
+// Phase B of variable v on the x-line x.l of element x.e.
+template <bool COH, class PB, class C = typename PB::C_t>
+__device__ __forceinline__ void stage_b_var(const PB& B, const BCtx<C>& x, int v) {
+    using S = typename PB::S_t;
+    using P = typename PB::P_t;
+    const Mesh& m = B.m;
     const bool defer = (B.flags & kDeferRK) != 0;
+    const long long e = x.e, nxm = x.nxm, nxp = x.nxp, nym = x.nym, nyp = x.nyp, nzm = x.nzm, nzp = x.nzp;
+    const int l = x.l, lj = x.lj, lk = x.lk;
+    const C hx = x.hx, hy = x.hy, hz = x.hz;
+    C acc[4] = {(C)0, (C)0, (C)0, (C)0};
+    // plus faces: the plus neighbours' minus-face records F_I - 1/2 Fv
+    {
+        const C f0 = ldf<COH>(B.fi + ((nxp * 3 + 0) * NV + v) * NF + l);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        C acc[4] = {(C)0, (C)0, (C)0, (C)0};
-        // plus faces: the plus neighbours' minus-face records F_I - 1/2 Fv
-        {
-            const C f0 = ldf<COH>(B.fi + ((nxp * 3 + 0) * NV + v) * NF + l);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(-B.jac[0] * B.tc.gR[i], f0, acc[i]);
-        }
-        if (nyp >= 0) {
-            C w[4];
-            ld4s(B.fi + ((nyp * 3 + 1) * NV + v) * NF + 4 * lk, w);
-            const C c = -B.jac[1] * B.tc.gR[lj];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
-        }
-        {
-            C w[4];
-            ld4s(B.fi + ((nzp * 3 + 2) * NV + v) * NF + 4 * lj, w);
-            const C c = -B.jac[2] * B.tc.gR[lk];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
-        }
-        if (v > 0) {
-            // minus faces: the minus neighbours' viscous fluxes at their plus faces
-            const int q = v - 1;
-            {
-                const C a0 = ldf<COH>(B.fv + ((nxm * 3 + 0) * 4 + q) * NF + l);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, acc[i]);
-            }
-            if (nym >= 0) {
-                C w[4];
-                ld4s(B.fv + ((nym * 3 + 1) * 4 + q) * NF + 4 * lk, w);
-                const C c = hy * B.tc.gL[lj];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
-            }
-            {
-                C w[4];
-                ld4s(B.fv + ((nzm * 3 + 2) * 4 + q) * NF + 4 * lj, w);
-                const C c = hz * B.tc.gL[lk];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
-            }
-        }
-        const long long off = v * m.npts + e * NE + 4 * l;
-        P out[4];
-        if (defer) {
-            C r[4];
-            P un[4], u0v[4];
-            if constexpr (COH)
-                ldc4<S, C>(B.rhs + off, r);
-            else
-                ldg4<S, C>(B.rhs + off, r);
-            ldg4<S, P>(B.u_in + off, un);
-            if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, u0v);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const C rt = r[i] + acc[i];
-                P o = B.rb * un[i] + B.rc * (P)rt;
-                if (B.flags & kHasU0) o = B.ra * u0v[i] + B.rb * un[i] + B.rc * (P)rt;
-                out[i] = o;
-            }
-        } else {
-            P cur[4];
-            ldc4<S, P>(B.u_out + off, cur);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) out[i] = cur[i] + B.rc * (P)acc[i];
-        }
-        // stored per variable: holding all five (20 more registers) cut the
-        // occupancy and measured 20% slower
-        stg4<S, P>(B.u_out + off, out);
+        for (int i = 0; i < 4; ++i) acc[i] = fma(-B.jac[0] * B.tc.gR[i], f0, acc[i]);
     }
+    if (nyp >= 0) {
+        C w[4];
+        ld4s(B.fi + ((nyp * 3 + 1) * NV + v) * NF + 4 * lk, w);
+        const C c = -B.jac[1] * B.tc.gR[lj];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+    }
+    {
+        C w[4];
+        ld4s(B.fi + ((nzp * 3 + 2) * NV + v) * NF + 4 * lj, w);
+        const C c = -B.jac[2] * B.tc.gR[lk];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+    }
+    if (v > 0) {
+        // minus faces: the minus neighbours' viscous fluxes at their plus faces
+        const int q = v - 1;
+        {
+            const C a0 = ldf<COH>(B.fv + ((nxm * 3 + 0) * 4 + q) * NF + l);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, acc[i]);
+        }
+        if (nym >= 0) {
+            C w[4];
+            ld4s(B.fv + ((nym * 3 + 1) * 4 + q) * NF + 4 * lk, w);
+            const C c = hy * B.tc.gL[lj];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+        }
+        {
+            C w[4];
+            ld4s(B.fv + ((nzm * 3 + 2) * 4 + q) * NF + 4 * lj, w);
+            const C c = hz * B.tc.gL[lk];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+        }
+    }
+    const long long off = v * m.npts + e * NE + 4 * l;
+    P out[4];
+    if (defer) {
+        C r[4];
+        P un[4], u0v[4];
+        if constexpr (COH)
+            ldc4<S, C>(B.rhs + off, r);
+        else
+            ldg4<S, C>(B.rhs + off, r);
+        ldg4<S, P>(B.u_in + off, un);
+        if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, u0v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const C rt = r[i] + acc[i];
+            P o = B.rb * un[i] + B.rc * (P)rt;
+            if (B.flags & kHasU0) o = B.ra * u0v[i] + B.rb * un[i] + B.rc * (P)rt;
+            out[i] = o;
+        }
+    } else {
+        P cur[4];
+        ldc4<S, P>(B.u_out + off, cur);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) out[i] = cur[i] + B.rc * (P)acc[i];
+    }
+    // stored per variable: holding all five (20 more registers) cut the
+    // occupancy and measured 20% slower
+    stg4<S, P>(B.u_out + off, out);
+}
+
+// One tile of phase B: EPB elements starting at B.e0 + tile * EPB, 16
+// threads (x-lines) each, all five variables per thread. COH: the face
+// buffers and the RHS were written by this same launch (a persistent kernel
+// after its grid barrier), so they are read through the coherent path.
+template <int EPB, bool COH, class PB>
+__device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
+    const int l = threadIdx.x & (LPE - 1);
+    const long long e = B.e0 + tile * EPB + threadIdx.x / LPE;
+    if (e >= B.e1) return;
+    const auto x = b_ctx(B, e, l);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) stage_b_var<COH>(B, x, v);
 }
 
 template <class S, class P, class C, int EPB>
 __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S, P, C> B) {
     stage_b_tile<EPB, false>(B, blockIdx.x);
+}
+
+// Phase B with one thread per (element, variable, x-line): 80 threads per
+// element; a warp holds two elements' lines of one variable.
+template <class S, class P, class C, int EPB>
+__global__ void __launch_bounds__(LPE * NV * EPB) stage_b_split_kernel(const StageBParams<S, P, C> B) {
+    const int g = threadIdx.x / LPE;
+    const int v = g / EPB;
+    const long long e = B.e0 + (long long)blockIdx.x * EPB + (g - v * EPB);
+    if (e >= B.e1) return;
+    stage_b_var<false>(B, b_ctx(B, e, threadIdx.x & (LPE - 1)), v);
 }
 
 }  // namespace od

@@ -131,7 +131,8 @@ def test_restart_bit_exact(prec):
 @pytest.mark.parametrize("prec", ["f32", "f64"])
 def test_slab_pipeline_and_launch_shape_do_not_change_results(prec):
     """The z-slab pipeline (phase B of a slab on a second stream) and the
-    phase-B block shape change scheduling only: byte-identical states. The
+    phase-B block shape (a thread per x-line or per x-line and variable)
+    change scheduling only: byte-identical states. The
     phase-A block shape (2 or 4 elements) selects another kernel, which the
     compiler may schedule with a multiply-add contracted differently: equal
     to round-off."""
@@ -141,7 +142,7 @@ def test_slab_pipeline_and_launch_shape_do_not_change_results(prec):
     _, dp = _pair(mesh, "slau2", True, prec)
     dt = float(np.float32(1e-3))
     outs = {}
-    for slabs, ea, eb in ((1, 4, 16), (2, 2, 8), (4, 4, 8), (8, 2, 16), (1, 2, 16)):
+    for slabs, ea, eb in ((1, 4, 16), (2, 2, 8), (4, 4, 8), (8, 2, 16), (1, 2, 16), (1, 4, 2), (2, 4, 4), (4, 2, 2)):
         with Solver(dp) as s:
             s.set_pipeline_slabs(slabs)
             s.set_launch_shape(ea, eb)
