@@ -431,6 +431,11 @@ int od_mlp_train_step(od_mlp* m, const void* Xpool, const void* Tpool, const lon
                       float lr, double* loss);
 /* input standardisation (x - mean) / scale per channel (14) and output scale per variable (5) */
 int od_mlp_set_scaling(od_mlp* m, const float* mean14, const float* scale14, const float* out_scale5);
+/* Inference inside an attached f32 solver as one fused kernel per stage (on,
+ * the default: all four layers per 128-element tile, activations kept in
+ * shared memory, output added into the RHS) or as four GEMM launches (off).
+ * Results agree to bf16 round-off of the same operands. */
+int od_mlp_set_fused(od_mlp* m, int on);
 /* Attach (m != null) or detach the network to a solver: every RK stage of
  * od_step then runs phase A, features of the stage's state, the network,
  * rhs += out_scale * output, phase B. Needs an f32 state. The network must

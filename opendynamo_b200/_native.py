@@ -31,6 +31,7 @@ EXPORTS = (
     "od_gemm_bf16",
     "od_mlp_create", "od_mlp_destroy", "od_mlp_last_error", "od_mlp_param_count", "od_mlp_set_params",
     "od_mlp_get_params", "od_mlp_forward", "od_mlp_gradients", "od_mlp_train_step", "od_mlp_set_scaling",
+    "od_mlp_set_fused",
     "od_attach_closure", "od_project", "od_closure_features", "od_f32_to_bf16",
     "od_point_fields", "od_fields_save", "od_xdmf_text", "od_xdmf_convert",
     "od_get_state_async", "od_create_slab", "od_slab_stage", "od_slab_halo_bytes", "od_slab_pack", "od_slab_unpack",
@@ -151,6 +152,7 @@ def lib() -> ctypes.CDLL:
         "od_mlp_gradients": (ci, [vp, vp, vp, vp, ci, ci, vp, ctypes.POINTER(cd)]),
         "od_mlp_train_step": (ci, [vp, vp, vp, vp, ci, ctypes.c_float, ctypes.POINTER(cd)]),
         "od_mlp_set_scaling": (ci, [vp, vp, vp, vp]),
+        "od_mlp_set_fused": (ci, [vp, ci]),
         "od_attach_closure": (ci, [vp, vp]),
         "od_project": (ci, [vp, ci, ci, ci, ci, ci, vp, ci, vp]),
         "od_closure_features": (ci, [vp, ci, ci, ci, ci, cd, cd, cd, vp, vp, vp, vp]),

@@ -329,6 +329,7 @@ struct od_mlp {
     std::string msg;
     // closure attachment (features of the coarse state + output scaling)
     float mean[kChan], scale[kChan], out_scale[5];
+    bool fused = true;       // inference as one kernel (mlp_fused_kernel) on an f32 state
     bf16* Xc = nullptr;      // features of the attached solver's elements
     float* Yc = nullptr;
     long long nelem_c = 0, mpad_c = 0;
@@ -612,6 +613,12 @@ int od_mlp_train_step(od_mlp* m, const void* Xpool, const void* Tpool, const lon
 }
 
 // Normalisation of the closure's inputs and outputs.
+int od_mlp_set_fused(od_mlp* m, int on) {
+    if (!m) return OD_ERR_ARG;
+    m->fused = on != 0;
+    return OD_OK;
+}
+
 int od_mlp_set_scaling(od_mlp* m, const float* mean14, const float* scale14, const float* out_scale5) {
     if (!m || !mean14 || !scale14 || !out_scale5) return OD_ERR_ARG;
     std::memcpy(m->mean, mean14, sizeof m->mean);
@@ -688,6 +695,23 @@ cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStre
     // out_scale * (output) into the RHS directly (f32 state)
     cudaStream_t keep = m->stream;
     m->stream = s;
+    if (e == cudaSuccess && m->fused && !m->attached_f64) {
+        // the whole network per 128-element tile in one kernel, output into the RHS
+        od::mlp::FusedArgs a{};
+        a.X = m->Xc;
+        for (int l = 0; l < 4; ++l) {
+            a.W[l] = m->wb[l];
+            a.bias[l] = m->w + m->off_b[l];
+        }
+        a.rhs = (float*)rhs;
+        a.rhs_npts = m->nelem_c * 64;
+        a.rhs_rows = (int)m->nelem_c;
+        for (int v = 0; v < 5; ++v) a.rhs_scale[v] = m->out_scale[v];
+        a.err = m->err;
+        e = od::mlp::launch_fused(a, (int)m->mpad_c, s);
+        m->stream = keep;
+        return e;
+    }
     if (e == cudaSuccess) e = hidden(m, m->Xc, (int)m->mpad_c, false);
     if (e == cudaSuccess) {
         if (m->attached_f64) {

@@ -7,6 +7,7 @@
 
 #include "../../include/opendynamo.h"
 #include "od_mlp.cuh"
+#include "od_mlp_fused.cuh"
 
 namespace od {
 namespace mlp {
@@ -91,6 +92,22 @@ cudaError_t launch_gemm(const GemmArgs& g0, int epi, cudaStream_t s, size_t ws_f
         case kApplyRhs: return launch_nt<kApplyRhs>(g, nt, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_fused(const FusedArgs& a, int M, cudaStream_t s) {
+    if (M <= 0 || M % BM) return cudaErrorInvalidValue;
+    static bool prepared[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!prepared[dev]) {
+        e = cudaFuncSetAttribute(mlp_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
+        if (e != cudaSuccess) return e;
+        prepared[dev] = true;
+    }
+    mlp_fused_kernel<<<(unsigned)(M / BM), kFThreads, fused_smem_bytes(), s>>>(a);
+    return cudaGetLastError();
 }
 
 }  // namespace mlp

@@ -7,13 +7,15 @@
 // over all of K or over one of `ksplit` K ranges (blockIdx.z; fp32 partial
 // tiles, summed by a second kernel):
 //   - all threads stage 128 x 64 (A) and NT x 64 (B) bf16 blocks into shared
-//     memory with 16-byte cp.async copies, two stages deep, in the canonical
+//     memory with 16-byte cp.async copies, three stages deep (two blocks in
+//     flight while the tensor cores work on a third), in the canonical
 //     no-swizzle K-major layout of the tensor cores: 8 x 16-byte core
 //     matrices, the two K halves of an MMA 128 B apart (LBO), 8-row groups
 //     1024 B apart (SBO);
 //   - thread 0 issues tcgen05.mma (kind::f16, M = 128, N = NT, K = 16) four
 //     times per 64-wide block into the TMEM accumulator and commits them to
-//     the stage's mbarrier, so the copy of block k+1 overlaps the MMAs of k;
+//     the stage's mbarrier, so the copies of blocks k+1 and k+2 overlap the
+//     MMAs of k;
 //   - the epilogue reads the accumulator with tcgen05.ld (warp w owns rows
 //     32w..32w+31, one row per thread) and applies one of the closure's
 //     fused epilogues (bias, GELU, GELU', transposed copies, fp32 store).
@@ -30,7 +32,7 @@ namespace mlp {
 
 constexpr int BM = 128;        // rows per CTA tile
 constexpr int BK = 64;         // K per pipeline stage
-constexpr int STAGES = 2;
+constexpr int STAGES = 3;
 constexpr long long kWaitLimit = 1LL << 26;
 
 enum Epi : int {
@@ -57,6 +59,22 @@ struct GemmArgs {
     int rhs_rows;             // elements (rows beyond are padding)
     float rhs_scale[5];
 };
+
+// Arguments of the fused inference kernel (od_mlp_fused.cuh): the whole
+// network on 128-row tiles, output added into the solver's RHS.
+struct FusedArgs {
+    const __nv_bfloat16* X;      // [M x 896] standardised features
+    const __nv_bfloat16* W[4];   // [256 x 896], [256 x 256], [256 x 256], [>= 320 x 256]
+    const float* bias[4];
+    float* rhs;                  // the solver's RHS: 5 planes of rhs_npts values
+    long long rhs_npts;
+    int rhs_rows;                // elements (rows beyond are padding)
+    float rhs_scale[5];
+    int* err;
+};
+
+// launches the fused inference kernel on M rows (a multiple of 128)
+cudaError_t launch_fused(const FusedArgs& a, int M, cudaStream_t s);
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -144,7 +162,6 @@ __device__ __forceinline__ void load_stage(const GemmArgs& g, Smem<NT>& s, int s
         const int kc = (c >> 3) & 7;
         cp_async16(smem_addr(s.b[st]) + tile_off(r, kc), g.B + (size_t)(n0 + r) * g.K + k0 + kc * 8);
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 template <int NT, int EPI>
@@ -180,11 +197,17 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
     const uint32_t tmem = s.tmem_base;
     const uint32_t idesc = instr_desc(BM, NT);
 
-    load_stage<NT>(g, s, 0, m0, n0, kb0);
+    // prologue: blocks 0 .. STAGES-2, one cp.async group each (empty groups
+    // past the end keep the group count equal to the block count)
+#pragma unroll
+    for (int i = 0; i < STAGES - 1; ++i) {
+        if (i < KB) load_stage<NT>(g, s, i, m0, n0, kb0 + i);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     for (int kb = 0; kb < KB; ++kb) {
         const int st = kb % STAGES;
-        // block kb has landed in stage st
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        // block kb has landed in stage st (at most STAGES-2 newer groups pending)
+        asm volatile("cp.async.wait_group %0;" ::"n"(STAGES - 2) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (t == 0 && !s.failed) {
@@ -205,9 +228,10 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
                              smem_addr(&s.bar[st]))
                          : "memory");
         }
-        // prefetch block kb+1 into the other stage once the MMAs that read it (block kb-1) are done
-        if (kb + 1 < KB) {
-            const int nst = (kb + 1) % STAGES;
+        // prefetch block kb+STAGES-1 into the stage of block kb-1 once its MMAs are done
+        const int nb = kb + STAGES - 1;
+        if (nb < KB) {
+            const int nst = nb % STAGES;
             if (kb >= 1) {
                 // completion number (kb-1)/STAGES of bar[nst]
                 const uint32_t parity = (uint32_t)(((kb - 1) / STAGES) & 1);
@@ -217,8 +241,9 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const GemmArgs g) {
                 }
             }
             __syncthreads();
-            if (!s.failed) load_stage<NT>(g, s, nst, m0, n0, kb0 + kb + 1);
+            if (!s.failed) load_stage<NT>(g, s, nst, m0, n0, kb0 + nb);
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
     }
     // all MMAs done: commit once more on the final barrier
     if (t == 0 && !s.failed) {

@@ -1,0 +1,276 @@
+// Fused closure inference on sm_100a (tcgen05 + TMEM): the whole per-element
+// network 896 -> 256 -> 256 -> 256 -> 320 for a tile of 128 elements in one
+// CTA, its output added straight into the solver's RHS.
+//
+// The hidden activations never leave the SM: each layer's epilogue reads the
+// accumulator from tensor memory (tcgen05.ld), adds the bias, applies GELU,
+// rounds to bf16 and writes the result into shared memory in the canonical
+// K-major core-matrix layout the next layer's MMAs read as their A operand.
+// Only the features (layer 1's A) and the weights (every layer's B, from L2)
+// are streamed, in 64-wide K blocks, three stages deep, with 16-byte cp.async;
+// thread 0 issues tcgen05.mma (kind::f16, M = 128, K = 16) and commits each
+// stage to its mbarrier. The output layer runs as two passes of N = 160
+// (columns 0-159 and 160-319: variables 0-2.5 and 2.5-5).
+//
+// Shared memory (224 KB): two 64 KB activation buffers of four 128 x 64
+// k-blocks each (the second also holds layer 1's three A stages) and three
+// 32 KB weight stages. Tensor memory: 256 fp32 columns, reused by every layer.
+// Every mbarrier wait is bounded: past the limit the CTA records an error,
+// skips the remaining work and frees its tensor memory.
+#pragma once
+
+#include "od_mlp.cuh"
+
+namespace od {
+namespace mlp {
+
+constexpr int kFIn = 896, kFHid = 256, kFOut = 320, kFPass = 160;
+constexpr int kFStages = 3;
+constexpr int kFThreads = 256;   // 8 warps: warp w reads TMEM lanes 32 (w % 4) .. +31, column half w / 4
+constexpr int kFSteps = kFIn / BK + 2 * (kFHid / BK) + 2 * (kFHid / BK);   // 14 + 4 + 4 + 2 x 4 = 30
+
+struct FusedSmem {
+    alignas(1024) unsigned char h[2][4][BM * BK * 2];   // activations [buffer][k-block]
+    alignas(1024) unsigned char b[kFStages][kFHid * BK * 2];   // weight stages
+    alignas(8) unsigned long long bar[kFStages];
+    alignas(8) unsigned long long done_bar;
+    uint32_t tmem_base;
+    int failed;
+};
+
+constexpr size_t fused_smem_bytes() { return sizeof(FusedSmem) + 1024; }
+
+// step -> (layer 0..3, pass of the output layer, K block)
+struct FStep {
+    int layer, pass, kb;
+};
+
+__device__ __forceinline__ FStep fused_step(int s) {
+    if (s < 14) return {0, 0, s};
+    if (s < 18) return {1, 0, s - 14};
+    if (s < 22) return {2, 0, s - 18};
+    return {3, (s - 22) >> 2, (s - 22) & 3};
+}
+
+// stage the weight block (and for layer 1 the feature block) of step s
+__device__ __forceinline__ void fused_load(const FusedArgs& g, FusedSmem& sm, int s, int m0) {
+    const FStep f = fused_step(s);
+    const int st = s % kFStages;
+    const int t = threadIdx.x;
+    const int K = f.layer == 0 ? kFIn : kFHid;
+    const int nrows = f.layer == 3 ? kFPass : kFHid;
+    const int n0 = f.layer == 3 ? f.pass * kFPass : 0;
+    const __nv_bfloat16* W = g.W[f.layer];
+    const int k0 = f.kb * BK;
+    for (int c = t; c < nrows * 8; c += kFThreads) {
+        const int r = (c & 7) + 8 * (c >> 6);
+        const int kc = (c >> 3) & 7;
+        cp_async16(smem_addr(sm.b[st]) + tile_off(r, kc), W + (size_t)(n0 + r) * K + k0 + kc * 8);
+    }
+    if (f.layer == 0) {
+#pragma unroll
+        for (int i = 0; i < (BM * 8) / kFThreads; ++i) {
+            const int c = t + kFThreads * i;
+            const int r = (c & 7) + 8 * (c >> 6);
+            const int kc = (c >> 3) & 7;
+            cp_async16(smem_addr(sm.h[1][st]) + tile_off(r, kc), g.X + (size_t)(m0 + r) * kFIn + k0 + kc * 8);
+        }
+    }
+}
+
+// 32 accumulator columns of this thread's row (TMEM lane) starting at column c
+__device__ __forceinline__ void fused_tmem_ld32(uint32_t lane_base, int c, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(lane_base + (uint32_t)c));
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(lane_base + (uint32_t)(c + 16)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// Epilogue of hidden layer l: bias + GELU -> bf16 rows into activation
+// buffer `out` (K-major tiles of 64 columns); each thread one row (its TMEM
+// lane) and one half of the columns.
+__device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedSmem& sm, int l, uint32_t tmem,
+                                                      unsigned char (*out)[BM * BK * 2]) {
+    const int t = threadIdx.x, warp = t >> 5, quarter = warp & 3, half = warp >> 2;
+    const int row = quarter * 32 + (t & 31);
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll 1
+    for (int c0 = half * (kFHid / 2); c0 < (half + 1) * (kFHid / 2); c0 += 32) {
+        float v[32];
+        fused_tmem_ld32(lane_base, c0, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t pk[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int j = 8 * q + 2 * h;
+                const __nv_bfloat162 p2 = __floats2bfloat162_rn(gelu(v[j] + g.bias[l][c0 + j]),
+                                                                gelu(v[j + 1] + g.bias[l][c0 + j + 1]));
+                pk[h] = *reinterpret_cast<const uint32_t*>(&p2);
+            }
+            const int n = c0 + 8 * q;
+            const uint32_t dst = smem_addr(out[n >> 6]) + tile_off(row, (n & 63) >> 3);
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(pk[0]), "r"(pk[1]), "r"(pk[2]),
+                         "r"(pk[3])
+                         : "memory");
+        }
+    }
+}
+
+// Epilogue of output pass p: rhs[var][row*64 + point] += scale[var] * (C + bias)
+// for the columns var*64 + point of this pass; rows through a per-warp 32 x 32
+// staging tile so that every update touches one contiguous row segment.
+__device__ __forceinline__ void fused_out_epilogue(const FusedArgs& g, FusedSmem& sm, int pass, uint32_t tmem,
+                                                   int m0) {
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, quarter = warp & 3, half = warp >> 2;
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+    // 8 warps x 4 KB in the second activation buffer, idle during the output layer
+    float* stg = reinterpret_cast<float*>(&sm.h[1][0][0]) + warp * 1024;
+    const int row0 = m0 + quarter * 32;
+#pragma unroll 1
+    for (int c0 = half * 32; c0 < kFPass; c0 += 64) {   // column chunks 0, 2, 4 | 1, 3
+        float v[32];
+        fused_tmem_ld32(lane_base, c0, v);
+        const int n = pass * kFPass + c0;   // 32 columns inside one variable's 64-point block
+        const int var = n >> 6;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j] + g.bias[3][n + j];
+        __syncwarp();
+        const float sc = g.rhs_scale[var];
+        float* base = g.rhs + (size_t)var * g.rhs_npts + (n & 63) + lane;
+        float cur[32];
+#pragma unroll
+        for (int rr = 0; rr < 32; ++rr) cur[rr] = row0 + rr < g.rhs_rows ? base[(size_t)(row0 + rr) * 64] : 0.f;
+#pragma unroll
+        for (int rr = 0; rr < 32; ++rr)
+            if (row0 + rr < g.rhs_rows) base[(size_t)(row0 + rr) * 64] = cur[rr] + sc * stg[rr * 32 + (lane ^ rr)];
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    FusedSmem& sm = *reinterpret_cast<FusedSmem*>(smem_raw + ((1024 - (smem_addr(smem_raw) & 1023)) & 1023));
+    const int t = threadIdx.x, warp = t >> 5;
+    const int m0 = blockIdx.x * BM;
+    constexpr uint32_t kCols = kFHid;
+
+    if (t == 0) {
+        for (int i = 0; i < kFStages; ++i) mbar_init(smem_addr(&sm.bar[i]), 1);
+        mbar_init(smem_addr(&sm.done_bar), 1);
+        sm.failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&sm.tmem_base)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem_base;
+
+    int done_count = 0;   // completions of done_bar so far (one per layer / output pass)
+    // prologue: steps 0 .. kFStages-2, one cp.async group each
+    for (int i = 0; i < kFStages - 1; ++i) {
+        fused_load(g, sm, i, m0);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (int s = 0; s < kFSteps; ++s) {
+        const FStep f = fused_step(s);
+        const int st = s % kFStages;
+        if (f.kb == 0 && s > 0) {
+            // the previous layer (or pass) is complete: its epilogue feeds this one
+            if (!sm.failed && !mbar_wait(smem_addr(&sm.done_bar), (uint32_t)(done_count & 1))) {
+                sm.failed = 1;
+                if (g.err) atomicExch(g.err, 1);
+            }
+            ++done_count;
+            __syncthreads();
+            const FStep p = fused_step(s - 1);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (!sm.failed) {
+                if (p.layer < 3)
+                    fused_hidden_epilogue(g, sm, p.layer, tmem, sm.h[p.layer & 1]);
+                else
+                    fused_out_epilogue(g, sm, p.pass, tmem, m0);
+            }
+            // generic-proxy writes of the activations -> visible to the MMAs
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        }
+        // step s has landed (at most kFStages-2 newer groups pending)
+        asm volatile("cp.async.wait_group %0;" ::"n"(kFStages - 2) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (t == 0 && !sm.failed) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int n = f.layer == 3 ? kFPass : kFHid;
+            const uint32_t idesc = instr_desc(BM, n);
+            const uint32_t a0 = f.layer == 0 ? smem_addr(sm.h[1][st]) : smem_addr(sm.h[(f.layer + 1) & 1][f.kb]);
+            const uint32_t b0 = smem_addr(sm.b[st]);
+#pragma unroll
+            for (int k = 0; k < BK / 16; ++k) {
+                const uint64_t ad = smem_desc(a0 + k * 256, 128, 1024);
+                const uint64_t bd = smem_desc(b0 + k * 256, 128, 1024);
+                const uint32_t acc = (f.kb > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&sm.bar[st]))
+                         : "memory");
+            const bool last = s + 1 == kFSteps || fused_step(s + 1).kb == 0;
+            if (last)
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_addr(&sm.done_bar))
+                             : "memory");
+        }
+        // prefetch step s+kFStages-1 into the stage of step s-1 once its MMAs are done
+        const int ns = s + kFStages - 1;
+        if (ns < kFSteps) {
+            if (s >= 1 && !sm.failed) {
+                const uint32_t parity = (uint32_t)(((s - 1) / kFStages) & 1);
+                if (!mbar_wait(smem_addr(&sm.bar[ns % kFStages]), parity)) {
+                    sm.failed = 1;
+                    if (g.err) atomicExch(g.err, 1);
+                }
+            }
+            __syncthreads();
+            if (!sm.failed) fused_load(g, sm, ns, m0);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    // the last output pass
+    bool ok = !sm.failed;
+    if (ok && !mbar_wait(smem_addr(&sm.done_bar), (uint32_t)(done_count & 1))) {
+        ok = false;
+        if (g.err) atomicExch(g.err, 1);
+    }
+    ok = __all_sync(0xffffffffu, ok);   // tcgen05.ld is warp-collective
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) fused_out_epilogue(g, sm, 1, tmem, m0);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+    }
+}
+
+}  // namespace mlp
+}  // namespace od
