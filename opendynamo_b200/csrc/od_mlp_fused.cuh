@@ -60,7 +60,8 @@ __device__ __forceinline__ void fused_load(const FusedArgs& g, FusedSmem& sm, in
     const int K = f.layer == 0 ? kFIn : kFHid;
     const int nrows = f.layer == 3 ? kFPass : kFHid;
     const int n0 = f.layer == 3 ? f.pass * kFPass : 0;
-    const __nv_bfloat16* W = g.W[f.layer];
+    // (selects: a parameter array indexed at run time would be copied to local memory)
+    const __nv_bfloat16* W = f.layer == 0 ? g.W[0] : f.layer == 1 ? g.W[1] : f.layer == 2 ? g.W[2] : g.W[3];
     const int k0 = f.kb * BK;
     for (int c = t; c < nrows * 8; c += kFThreads) {
         const int r = (c & 7) + 8 * (c >> 6);
@@ -104,6 +105,7 @@ __device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedS
     const int t = threadIdx.x, warp = t >> 5, quarter = warp & 3, half = warp >> 2;
     const int row = quarter * 32 + (t & 31);
     const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+    const float* bias = l == 0 ? g.bias[0] : l == 1 ? g.bias[1] : g.bias[2];
 #pragma unroll 1
     for (int c0 = half * (kFHid / 2); c0 < (half + 1) * (kFHid / 2); c0 += 32) {
         float v[32];
@@ -114,8 +116,8 @@ __device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedS
 #pragma unroll
             for (int h = 0; h < 4; ++h) {
                 const int j = 8 * q + 2 * h;
-                const __nv_bfloat162 p2 = __floats2bfloat162_rn(gelu(v[j] + g.bias[l][c0 + j]),
-                                                                gelu(v[j + 1] + g.bias[l][c0 + j + 1]));
+                const __nv_bfloat162 p2 = __floats2bfloat162_rn(gelu(v[j] + bias[c0 + j]),
+                                                                gelu(v[j + 1] + bias[c0 + j + 1]));
                 pk[h] = *reinterpret_cast<const uint32_t*>(&p2);
             }
             const int n = c0 + 8 * q;
@@ -129,7 +131,8 @@ __device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedS
 
 // Epilogue of output pass p: rhs[var][row*64 + point] += scale[var] * (C + bias)
 // for the columns var*64 + point of this pass; rows through a per-warp 32 x 32
-// staging tile so that every update touches one contiguous row segment.
+// staging tile so that every reduction instruction covers one contiguous row
+// segment.
 __device__ __forceinline__ void fused_out_epilogue(const FusedArgs& g, FusedSmem& sm, int pass, uint32_t tmem,
                                                    int m0) {
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, quarter = warp & 3, half = warp >> 2;
@@ -146,14 +149,14 @@ __device__ __forceinline__ void fused_out_epilogue(const FusedArgs& g, FusedSmem
 #pragma unroll
         for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j] + g.bias[3][n + j];
         __syncwarp();
-        const float sc = g.rhs_scale[var];
+        const float sc = var == 0 ? g.rhs_scale[0] : var == 1 ? g.rhs_scale[1] : var == 2 ? g.rhs_scale[2]
+                       : var == 3 ? g.rhs_scale[3] : g.rhs_scale[4];
         float* base = g.rhs + (size_t)var * g.rhs_npts + (n & 63) + lane;
-        float cur[32];
-#pragma unroll
-        for (int rr = 0; rr < 32; ++rr) cur[rr] = row0 + rr < g.rhs_rows ? base[(size_t)(row0 + rr) * 64] : 0.f;
+        // one reduction per RHS value (a single contribution each: the same
+        // rounding as load + add + store, without the load's round trip)
 #pragma unroll
         for (int rr = 0; rr < 32; ++rr)
-            if (row0 + rr < g.rhs_rows) base[(size_t)(row0 + rr) * 64] = cur[rr] + sc * stg[rr * 32 + (lane ^ rr)];
+            if (row0 + rr < g.rhs_rows) atomicAdd(base + (size_t)(row0 + rr) * 64, sc * stg[rr * 32 + (lane ^ rr)]);
         __syncwarp();
     }
 }
