@@ -407,7 +407,7 @@ def run_closure_step(args, world, rank, local):
     return {"metric": f"closure step cost, channel {n}^3 (ms per SSP-RK3 step)", "value": round(out["closure"], 4),
             "unit": "ms/step", "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": False,
             "dtype": "f32 solver / bf16 network", "data": "synthetic (channel trip IC, random network)",
-            "config": {"workload": f"channel {n}^3, SLAU2, per-stage features + 4 tcgen05 GEMMs",
+            "config": {"workload": f"channel {n}^3, SLAU2, per-stage features + fused tcgen05 network kernel",
                        "form": "closure-step"},
             "plain_ms_per_step": round(out["plain"], 4),
             "closure_gdof_stage_s": round(npts * 3 / (out["closure"] / 1e3) / 1e9, 3)}
