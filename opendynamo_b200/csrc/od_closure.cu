@@ -312,6 +312,7 @@ struct od_mlp {
     long long off_w[4], off_b[4];
     int rows[4], cols[4];
     bf16 *wb[4] = {}, *wbT[4] = {};
+    bf16* wt = nullptr;   // the fused inference kernel's weight image (refreshed with wb)
     // activations
     float* Z[3] = {};
     bf16 *A[3] = {}, *AT[3] = {};
@@ -471,6 +472,7 @@ int od_mlp_create(int max_rows, int device, od_mlp** out) {
         mal((void**)&m->wb[l], sizeof(bf16) * R[l] * C[l]);
         mal((void**)&m->wbT[l], sizeof(bf16) * R[l] * C[l]);
     }
+    mal((void**)&m->wt, od::mlp::kFusedWeightBytes);
     for (int l = 0; l < 3; ++l) {
         mal((void**)&m->Z[l], sizeof(float) * M * kHid);
         mal((void**)&m->A[l], sizeof(bf16) * M * kHid);
@@ -502,7 +504,7 @@ void od_mlp_destroy(od_mlp* m) {
     void* ps[] = {m->w, m->m1, m->m2, m->g, m->wb[0], m->wb[1], m->wb[2], m->wb[3], m->wbT[0], m->wbT[1], m->wbT[2],
                   m->wbT[3], m->Z[0], m->Z[1], m->Z[2], m->A[0], m->A[1], m->A[2], m->AT[0], m->AT[1], m->AT[2],
                   m->Y, m->dY, m->dYT, m->dZa, m->dZaT, m->dZb, m->dZbT, m->X, m->XT, m->T, m->rows_d, m->loss,
-                  m->err, m->Xc, m->Yc, m->ws};
+                  m->err, m->Xc, m->Yc, m->ws, m->wt};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -528,6 +530,7 @@ int od_mlp_set_params(od_mlp* m, const float* host) {
                                                                     m->wb[l], m->wbT[l]);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = od::mlp::tile_fused_weights(m->wb, m->wt, m->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
     m->step = 0;
     if (e != cudaSuccess) return mfail(m, OD_ERR_CUDA, cudaGetErrorString(e));
@@ -604,6 +607,7 @@ int od_mlp_train_step(od_mlp* m, const void* Xpool, const void* Tpool, const lon
                                                                      m->rows[l], nullptr, nullptr);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = od::mlp::tile_fused_weights(m->wb, m->wt, m->stream);
     double l = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&l, m->loss, sizeof(double), cudaMemcpyDeviceToHost, m->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
@@ -699,8 +703,8 @@ cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStre
         // the whole network per 128-element tile in one kernel, output into the RHS
         od::mlp::FusedArgs a{};
         a.X = m->Xc;
+        a.Wt = m->wt;
         for (int l = 0; l < 4; ++l) {
-            a.W[l] = m->wb[l];
             a.bias[l] = m->w + m->off_b[l];
         }
         a.rhs = (float*)rhs;

@@ -94,6 +94,37 @@ cudaError_t launch_gemm(const GemmArgs& g0, int epi, cudaStream_t s, size_t ws_f
     }
 }
 
+__global__ void tile_fused_weights_kernel(const __nv_bfloat16* __restrict__ W0, const __nv_bfloat16* __restrict__ W1,
+                                          const __nv_bfloat16* __restrict__ W2, const __nv_bfloat16* __restrict__ W3,
+                                          __nv_bfloat16* __restrict__ Wt) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;   // 16-byte chunk of the image
+    if (q >= kFusedWeightBytes / 16) return;
+    const uint32_t byte = q * 16;
+    int s;
+    uint32_t within;
+    if (byte < 22u * kFStageBytes) {
+        s = (int)(byte / kFStageBytes);
+        within = byte % kFStageBytes;
+    } else {
+        s = 22 + (int)((byte - 22u * kFStageBytes) / kFOutStageBytes);
+        within = (byte - 22u * kFStageBytes) % kFOutStageBytes;
+    }
+    const FStep f = fused_step(s);
+    const int r = (int)(within / 1024) * 8 + (int)(within % 128) / 16;   // inverse of tile_off
+    const int kc = (int)(within % 1024) / 128;
+    const int K = f.layer == 0 ? kFIn : kFHid;
+    const int n0 = f.layer == 3 ? f.pass * kFPass : 0;
+    const __nv_bfloat16* W = f.layer == 0 ? W0 : f.layer == 1 ? W1 : f.layer == 2 ? W2 : W3;
+    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(Wt) + byte) =
+        *reinterpret_cast<const uint4*>(W + (size_t)(n0 + r) * K + f.kb * BK + kc * 8);
+}
+
+cudaError_t tile_fused_weights(const __nv_bfloat16* const W[4], __nv_bfloat16* Wt, cudaStream_t s) {
+    constexpr unsigned n = (unsigned)(kFusedWeightBytes / 16);
+    tile_fused_weights_kernel<<<(n + 255) / 256, 256, 0, s>>>(W[0], W[1], W[2], W[3], Wt);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fused(const FusedArgs& a, int M, cudaStream_t s) {
     if (M <= 0 || M % BM) return cudaErrorInvalidValue;
     static bool prepared[64] = {};

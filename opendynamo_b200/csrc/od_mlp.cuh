@@ -64,7 +64,7 @@ struct GemmArgs {
 // network on 128-row tiles, output added into the solver's RHS.
 struct FusedArgs {
     const __nv_bfloat16* X;      // [M x 896] standardised features
-    const __nv_bfloat16* W[4];   // [256 x 896], [256 x 256], [256 x 256], [>= 320 x 256]
+    const __nv_bfloat16* Wt;     // the weights in step order and shared-memory layout (tile_fused_weights)
     const float* bias[4];
     float* rhs;                  // the solver's RHS: 5 planes of rhs_npts values
     long long rhs_npts;
@@ -75,6 +75,15 @@ struct FusedArgs {
 
 // launches the fused inference kernel on M rows (a multiple of 128)
 cudaError_t launch_fused(const FusedArgs& a, int M, cudaStream_t s);
+
+// bytes of the fused kernel's weight image
+constexpr size_t kFusedWeightBytes = 884736;
+
+// writes the weight image the fused kernel streams: for each of its 30 K
+// steps the B tile (256 or 160 rows x 64 columns of one layer) in the
+// shared-memory core-matrix layout, so that one bulk copy fills a stage.
+// W: [256 x 896], [256 x 256], [256 x 256], [>= 320 x 256] bf16.
+cudaError_t tile_fused_weights(const __nv_bfloat16* const W[4], __nv_bfloat16* Wt, cudaStream_t s);
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));

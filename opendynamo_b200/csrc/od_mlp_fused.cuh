@@ -7,14 +7,21 @@
 // rounds to bf16 and writes the result into shared memory in the canonical
 // K-major core-matrix layout the next layer's MMAs read as their A operand.
 // Only the features (layer 1's A) and the weights (every layer's B, from L2)
-// are streamed, in 64-wide K blocks, three stages deep, with 16-byte cp.async;
-// thread 0 issues tcgen05.mma (kind::f16, M = 128, K = 16) and commits each
-// stage to its mbarrier. The output layer runs as two passes of N = 160
+// are streamed, in 64-wide K blocks, four stages deep: the weights as one
+// bulk copy per stage from a step-ordered image already in the shared-memory
+// layout (tile_fused_weights), completing on the stage's `full` mbarrier; the
+// features with 16-byte cp.async by all threads. Thread 0 issues the bulk
+// copies and tcgen05.mma (kind::f16, M = 128, K = 16) and commits each stage's
+// MMAs to its `bar` mbarrier. The output layer runs as two passes of N = 160
 // (columns 0-159 and 160-319: variables 0-2.5 and 2.5-5).
 //
-// Shared memory (224 KB): two 64 KB activation buffers of four 128 x 64
-// k-blocks each (the second also holds layer 1's three A stages) and three
-// 32 KB weight stages. Tensor memory: 256 fp32 columns, reused by every layer.
+// Shared memory (209 KB): one 64 KB activation buffer of four 128 x 64
+// k-blocks, four 32 KB weight stages and a 17 KB staging area for the RHS
+// update. A layer's epilogue overwrites its own input in place: it starts
+// only after all of the layer's MMAs have completed. During layer 1 the
+// activation buffer holds the four feature stages instead (layer 1's output
+// is written after its last MMA). Tensor memory: 256 fp32 columns, reused by
+// every layer.
 // Every mbarrier wait is bounded: past the limit the CTA records an error,
 // skips the remaining work and frees its tensor memory.
 #pragma once
@@ -25,14 +32,20 @@ namespace od {
 namespace mlp {
 
 constexpr int kFIn = 896, kFHid = 256, kFOut = 320, kFPass = 160;
-constexpr int kFStages = 3;
+constexpr int kFStages = 4;
 constexpr int kFThreads = 256;   // 8 warps: warp w reads TMEM lanes 32 (w % 4) .. +31, column half w / 4
 constexpr int kFSteps = kFIn / BK + 2 * (kFHid / BK) + 2 * (kFHid / BK);   // 14 + 4 + 4 + 2 x 4 = 30
+constexpr uint32_t kFStageBytes = kFHid * BK * 2;      // weight tile of a hidden-layer step
+constexpr uint32_t kFOutStageBytes = kFPass * BK * 2;  // weight tile of an output step
+static_assert(22 * kFStageBytes + 8 * kFOutStageBytes == kFusedWeightBytes, "weight image size");
 
 struct FusedSmem {
-    alignas(1024) unsigned char h[2][4][BM * BK * 2];   // activations [buffer][k-block]
+    alignas(1024) unsigned char h[4][BM * BK * 2];   // activations [k-block]; layer 1: feature stages
     alignas(1024) unsigned char b[kFStages][kFHid * BK * 2];   // weight stages
-    alignas(8) unsigned long long bar[kFStages];
+    alignas(16) float stg[kFThreads / 32][32 * 17];   // per-warp 32 x 16 staging tile (row stride 17)
+    alignas(16) float bias[3 * kFHid + kFOut];   // the four layers' biases, read by every epilogue
+    alignas(8) unsigned long long bar[kFStages];    // the stage's MMAs are complete (stage free)
+    alignas(8) unsigned long long full[kFStages];   // the stage's weight tile has landed
     alignas(8) unsigned long long done_bar;
     uint32_t tmem_base;
     int failed;
@@ -52,30 +65,36 @@ __device__ __forceinline__ FStep fused_step(int s) {
     return {3, (s - 22) >> 2, (s - 22) & 3};
 }
 
-// stage the weight block (and for layer 1 the feature block) of step s
-__device__ __forceinline__ void fused_load(const FusedArgs& g, FusedSmem& sm, int s, int m0) {
-    const FStep f = fused_step(s);
+// byte offset of step s's weight tile in the image, and its size
+__device__ __forceinline__ uint32_t fused_w_off(int s) {
+    return s < 22 ? (uint32_t)s * kFStageBytes : 22u * kFStageBytes + (uint32_t)(s - 22) * kFOutStageBytes;
+}
+__device__ __forceinline__ uint32_t fused_w_bytes(int s) { return s < 22 ? kFStageBytes : kFOutStageBytes; }
+
+// thread 0: the weight tile of step s into its stage, one bulk copy that
+// completes on the stage's `full` barrier
+__device__ __forceinline__ void fused_load_w(const FusedArgs& g, FusedSmem& sm, int s) {
+    const int st = s % kFStages;
+    const uint32_t bar = smem_addr(&sm.full[st]);
+    const uint32_t bytes = fused_w_bytes(s);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(sm.b[st])),
+                 "l"(reinterpret_cast<const char*>(g.Wt) + fused_w_off(s)), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// all threads: the feature block of a layer-1 step
+__device__ __forceinline__ void fused_load_x(const FusedArgs& g, FusedSmem& sm, int s, int m0) {
     const int st = s % kFStages;
     const int t = threadIdx.x;
-    const int K = f.layer == 0 ? kFIn : kFHid;
-    const int nrows = f.layer == 3 ? kFPass : kFHid;
-    const int n0 = f.layer == 3 ? f.pass * kFPass : 0;
-    // (selects: a parameter array indexed at run time would be copied to local memory)
-    const __nv_bfloat16* W = f.layer == 0 ? g.W[0] : f.layer == 1 ? g.W[1] : f.layer == 2 ? g.W[2] : g.W[3];
-    const int k0 = f.kb * BK;
-    for (int c = t; c < nrows * 8; c += kFThreads) {
+    const int k0 = s * BK;
+#pragma unroll
+    for (int i = 0; i < (BM * 8) / kFThreads; ++i) {
+        const int c = t + kFThreads * i;
         const int r = (c & 7) + 8 * (c >> 6);
         const int kc = (c >> 3) & 7;
-        cp_async16(smem_addr(sm.b[st]) + tile_off(r, kc), W + (size_t)(n0 + r) * K + k0 + kc * 8);
-    }
-    if (f.layer == 0) {
-#pragma unroll
-        for (int i = 0; i < (BM * 8) / kFThreads; ++i) {
-            const int c = t + kFThreads * i;
-            const int r = (c & 7) + 8 * (c >> 6);
-            const int kc = (c >> 3) & 7;
-            cp_async16(smem_addr(sm.h[1][st]) + tile_off(r, kc), g.X + (size_t)(m0 + r) * kFIn + k0 + kc * 8);
-        }
+        cp_async16(smem_addr(sm.h[st]) + tile_off(r, kc), g.X + (size_t)(m0 + r) * kFIn + k0 + kc * 8);
     }
 }
 
@@ -97,31 +116,49 @@ __device__ __forceinline__ void fused_tmem_ld32(uint32_t lane_base, int c, float
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-// Epilogue of hidden layer l: bias + GELU -> bf16 rows into activation
-// buffer `out` (K-major tiles of 64 columns); each thread one row (its TMEM
-// lane) and one half of the columns.
-__device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedSmem& sm, int l, uint32_t tmem,
-                                                      unsigned char (*out)[BM * BK * 2]) {
+// 64 accumulator columns of this thread's row starting at column c, one wait
+__device__ __forceinline__ void fused_tmem_ld64(uint32_t lane_base, int c, float* v) {
+    uint32_t r[64];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[16 * q + 0]), "=r"(r[16 * q + 1]), "=r"(r[16 * q + 2]), "=r"(r[16 * q + 3]), "=r"(r[16 * q + 4]),
+              "=r"(r[16 * q + 5]), "=r"(r[16 * q + 6]), "=r"(r[16 * q + 7]), "=r"(r[16 * q + 8]), "=r"(r[16 * q + 9]),
+              "=r"(r[16 * q + 10]), "=r"(r[16 * q + 11]), "=r"(r[16 * q + 12]), "=r"(r[16 * q + 13]),
+              "=r"(r[16 * q + 14]), "=r"(r[16 * q + 15])
+            : "r"(lane_base + (uint32_t)(c + 16 * q)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// Epilogue of hidden layer l: bias + GELU -> bf16 rows into the activation
+// buffer (K-major tiles of 64 columns); each thread one row (its TMEM lane)
+// and one half of the columns.
+__device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedSmem& sm, int l, uint32_t tmem) {
     const int t = threadIdx.x, warp = t >> 5, quarter = warp & 3, half = warp >> 2;
     const int row = quarter * 32 + (t & 31);
     const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
-    const float* bias = l == 0 ? g.bias[0] : l == 1 ? g.bias[1] : g.bias[2];
+    const float* bias = sm.bias + l * kFHid;
 #pragma unroll 1
-    for (int c0 = half * (kFHid / 2); c0 < (half + 1) * (kFHid / 2); c0 += 32) {
-        float v[32];
-        fused_tmem_ld32(lane_base, c0, v);
+    for (int c0 = half * (kFHid / 2); c0 < (half + 1) * (kFHid / 2); c0 += 64) {
+        float v[64];
+        fused_tmem_ld64(lane_base, c0, v);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 8; ++q) {
+            const float4 b0 = *reinterpret_cast<const float4*>(bias + c0 + 8 * q);
+            const float4 b1 = *reinterpret_cast<const float4*>(bias + c0 + 8 * q + 4);
+            const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
             uint32_t pk[4];
 #pragma unroll
             for (int h = 0; h < 4; ++h) {
                 const int j = 8 * q + 2 * h;
-                const __nv_bfloat162 p2 = __floats2bfloat162_rn(gelu(v[j] + bias[c0 + j]),
-                                                                gelu(v[j + 1] + bias[c0 + j + 1]));
+                const __nv_bfloat162 p2 = __floats2bfloat162_rn(gelu(v[j] + bb[2 * h]), gelu(v[j + 1] + bb[2 * h + 1]));
                 pk[h] = *reinterpret_cast<const uint32_t*>(&p2);
             }
             const int n = c0 + 8 * q;
-            const uint32_t dst = smem_addr(out[n >> 6]) + tile_off(row, (n & 63) >> 3);
+            const uint32_t dst = smem_addr(sm.h[n >> 6]) + tile_off(row, (n & 63) >> 3);
             asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(pk[0]), "r"(pk[1]), "r"(pk[2]),
                          "r"(pk[3])
                          : "memory");
@@ -130,34 +167,39 @@ __device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedS
 }
 
 // Epilogue of output pass p: rhs[var][row*64 + point] += scale[var] * (C + bias)
-// for the columns var*64 + point of this pass; rows through a per-warp 32 x 32
-// staging tile so that every reduction instruction covers one contiguous row
-// segment.
+// for the columns var*64 + point of this pass; 16 columns at a time through
+// the warp's staging tile, so that every reduction instruction covers two
+// contiguous 64-byte row segments.
 __device__ __forceinline__ void fused_out_epilogue(const FusedArgs& g, FusedSmem& sm, int pass, uint32_t tmem,
                                                    int m0) {
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, quarter = warp & 3, half = warp >> 2;
     const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
-    // 8 warps x 4 KB in the second activation buffer, idle during the output layer
-    float* stg = reinterpret_cast<float*>(&sm.h[1][0][0]) + warp * 1024;
+    float* stg = sm.stg[warp];
     const int row0 = m0 + quarter * 32;
+    const int sub = lane >> 4, col = lane & 15;
 #pragma unroll 1
     for (int c0 = half * 32; c0 < kFPass; c0 += 64) {   // column chunks 0, 2, 4 | 1, 3
         float v[32];
         fused_tmem_ld32(lane_base, c0, v);
         const int n = pass * kFPass + c0;   // 32 columns inside one variable's 64-point block
         const int var = n >> 6;
-#pragma unroll
-        for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j] + g.bias[3][n + j];
-        __syncwarp();
         const float sc = var == 0 ? g.rhs_scale[0] : var == 1 ? g.rhs_scale[1] : var == 2 ? g.rhs_scale[2]
                        : var == 3 ? g.rhs_scale[3] : g.rhs_scale[4];
-        float* base = g.rhs + (size_t)var * g.rhs_npts + (n & 63) + lane;
-        // one reduction per RHS value (a single contribution each: the same
-        // rounding as load + add + store, without the load's round trip)
 #pragma unroll
-        for (int rr = 0; rr < 32; ++rr)
-            if (row0 + rr < g.rhs_rows) atomicAdd(base + (size_t)(row0 + rr) * 64, sc * stg[rr * 32 + (lane ^ rr)]);
-        __syncwarp();
+        for (int hh = 0; hh < 2; ++hh) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = v[16 * hh + j] + sm.bias[3 * kFHid + n + 16 * hh + j];
+            __syncwarp();
+            float* base = g.rhs + (size_t)var * g.rhs_npts + (n & 63) + 16 * hh + col;
+            // one reduction per RHS value (a single contribution each: the same
+            // rounding as load + add + store, without the load's round trip)
+#pragma unroll
+            for (int rr = 0; rr < 32; rr += 2) {
+                const int r = rr + sub;
+                if (row0 + r < g.rhs_rows) atomicAdd(base + (size_t)(row0 + r) * 64, sc * stg[r * 17 + col]);
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -169,7 +211,10 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
     constexpr uint32_t kCols = kFHid;
 
     if (t == 0) {
-        for (int i = 0; i < kFStages; ++i) mbar_init(smem_addr(&sm.bar[i]), 1);
+        for (int i = 0; i < kFStages; ++i) {
+            mbar_init(smem_addr(&sm.bar[i]), 1);
+            mbar_init(smem_addr(&sm.full[i]), 1);
+        }
         mbar_init(smem_addr(&sm.done_bar), 1);
         sm.failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -185,10 +230,18 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem_base;
 
+    for (int i = t; i < 3 * kFHid + kFOut; i += kFThreads)
+        sm.bias[i] = i < kFHid ? g.bias[0][i] : i < 2 * kFHid ? g.bias[1][i - kFHid]
+                   : i < 3 * kFHid ? g.bias[2][i - 2 * kFHid] : g.bias[3][i - 3 * kFHid];
     int done_count = 0;   // completions of done_bar so far (one per layer / output pass)
+    int w_issued = 0, w_landed = 0;   // thread 0: weight tiles requested / seen complete
     // prologue: steps 0 .. kFStages-2, one cp.async group each
     for (int i = 0; i < kFStages - 1; ++i) {
-        fused_load(g, sm, i, m0);
+        if (t == 0) {
+            fused_load_w(g, sm, i);
+            ++w_issued;
+        }
+        fused_load_x(g, sm, i, m0);
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
     for (int s = 0; s < kFSteps; ++s) {
@@ -206,7 +259,7 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!sm.failed) {
                 if (p.layer < 3)
-                    fused_hidden_epilogue(g, sm, p.layer, tmem, sm.h[p.layer & 1]);
+                    fused_hidden_epilogue(g, sm, p.layer, tmem);
                 else
                     fused_out_epilogue(g, sm, p.pass, tmem, m0);
             }
@@ -219,10 +272,18 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (t == 0 && !sm.failed) {
+            if (mbar_wait(smem_addr(&sm.full[st]), (uint32_t)((s / kFStages) & 1))) {
+                ++w_landed;
+            } else {
+                sm.failed = 1;
+                if (g.err) atomicExch(g.err, 1);
+            }
+        }
+        if (t == 0 && !sm.failed) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int n = f.layer == 3 ? kFPass : kFHid;
             const uint32_t idesc = instr_desc(BM, n);
-            const uint32_t a0 = f.layer == 0 ? smem_addr(sm.h[1][st]) : smem_addr(sm.h[(f.layer + 1) & 1][f.kb]);
+            const uint32_t a0 = smem_addr(sm.h[f.layer == 0 ? st : f.kb]);
             const uint32_t b0 = smem_addr(sm.b[st]);
 #pragma unroll
             for (int k = 0; k < BK / 16; ++k) {
@@ -255,7 +316,13 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
                 }
             }
             __syncthreads();
-            if (!sm.failed) fused_load(g, sm, ns, m0);
+            if (!sm.failed) {
+                if (t == 0) {
+                    fused_load_w(g, sm, ns);
+                    ++w_issued;
+                }
+                if (ns < kFIn / BK) fused_load_x(g, sm, ns, m0);
+            }
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
@@ -268,6 +335,14 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
     ok = __all_sync(0xffffffffu, ok);   // tcgen05.ld is warp-collective
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) fused_out_epilogue(g, sm, 1, tmem, m0);
+    // no copy may still be writing this CTA's shared memory when it exits (only
+    // after a failed wait are there requested tiles that no MMA consumed)
+    if (t == 0) {
+        for (int s = w_landed; s < w_issued; ++s)
+            if (!mbar_wait(smem_addr(&sm.full[s % kFStages]), (uint32_t)((s / kFStages) & 1)) && g.err)
+                atomicExch(g.err, 1);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
