@@ -128,7 +128,11 @@ struct FeatParams {
     float mean[kChan], inv_scale[kChan];
 };
 
-template <class T>
+// X: row-major [element][channel * 64 + point], or (TILED) the fused
+// inference kernel's layout: per 128-element tile, per channel (one 64-wide
+// K block) the 128 x 64 block in the shared-memory core-matrix layout, so
+// that one bulk copy fills a feature stage.
+template <class T, bool TILED = false>
 __global__ void __launch_bounds__(64) features_kernel(const T* __restrict__ u, FeatParams fp, bf16* __restrict__ X) {
     __shared__ float q[4][64];
     const long long e = blockIdx.x;
@@ -162,11 +166,13 @@ __global__ void __launch_bounds__(64) features_kernel(const T* __restrict__ u, F
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b) ch[5 + 3 * a + b] = (d[1 + a][b] - c[1 + a] * ir * d[0][b]) * ir;
-    bf16* row = X + e * kIn;
+    bf16* row = TILED ? X + (e >> 7) * (128 * kIn) + od::mlp::tile_off((int)(e & 127), p >> 3) / 2 + (p & 7)
+                      : X + e * kIn + p;
+    constexpr int kStride = TILED ? 128 * 64 : 64;   // elements between channels
 #pragma unroll
     for (int ch_i = 0; ch_i < kChan; ++ch_i)
-        row[ch_i * 64 + p] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i],
-                                                             -kClip), kClip));
+        row[ch_i * kStride] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i],
+                                                              -kClip), kClip));
 }
 
 FeatParams feat_params(int nx, int ny, int nz, double lx, double ly, double lz, const float* mean,
@@ -692,6 +698,8 @@ cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStre
     cudaError_t e = cudaSuccess;
     if (m->attached_f64)
         features_kernel<double><<<(unsigned)m->nelem_c, 64, 0, s>>>((const double*)u_in, m->fp, m->Xc);
+    else if (m->fused)
+        features_kernel<float, true><<<(unsigned)m->nelem_c, 64, 0, s>>>((const float*)u_in, m->fp, m->Xc);
     else
         features_kernel<float><<<(unsigned)m->nelem_c, 64, 0, s>>>((const float*)u_in, m->fp, m->Xc);
     e = cudaGetLastError();

@@ -71,31 +71,29 @@ __device__ __forceinline__ uint32_t fused_w_off(int s) {
 }
 __device__ __forceinline__ uint32_t fused_w_bytes(int s) { return s < 22 ? kFStageBytes : kFOutStageBytes; }
 
-// thread 0: the weight tile of step s into its stage, one bulk copy that
-// completes on the stage's `full` barrier
-__device__ __forceinline__ void fused_load_w(const FusedArgs& g, FusedSmem& sm, int s) {
+constexpr uint32_t kFXBytes = BM * BK * 2;   // feature block of a layer-1 step
+
+// thread 0: the weight tile of step s (and for layer 1 the tile's feature
+// block) into its stage, bulk copies that complete on the stage's `full`
+// barrier
+__device__ __forceinline__ void fused_load(const FusedArgs& g, FusedSmem& sm, int s, int tile) {
     const int st = s % kFStages;
     const uint32_t bar = smem_addr(&sm.full[st]);
-    const uint32_t bytes = fused_w_bytes(s);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    const uint32_t wbytes = fused_w_bytes(s);
+    const bool feat = s < kFIn / BK;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"(wbytes + (feat ? kFXBytes : 0u))
+                 : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_addr(sm.b[st])),
-                 "l"(reinterpret_cast<const char*>(g.Wt) + fused_w_off(s)), "r"(bytes), "r"(bar)
+                 "l"(reinterpret_cast<const char*>(g.Wt) + fused_w_off(s)), "r"(wbytes), "r"(bar)
                  : "memory");
-}
-
-// all threads: the feature block of a layer-1 step
-__device__ __forceinline__ void fused_load_x(const FusedArgs& g, FusedSmem& sm, int s, int m0) {
-    const int st = s % kFStages;
-    const int t = threadIdx.x;
-    const int k0 = s * BK;
-#pragma unroll
-    for (int i = 0; i < (BM * 8) / kFThreads; ++i) {
-        const int c = t + kFThreads * i;
-        const int r = (c & 7) + 8 * (c >> 6);
-        const int kc = (c >> 3) & 7;
-        cp_async16(smem_addr(sm.h[st]) + tile_off(r, kc), g.X + (size_t)(m0 + r) * kFIn + k0 + kc * 8);
-    }
+    if (feat)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(sm.h[st])),
+                     "l"(reinterpret_cast<const char*>(g.X) + ((size_t)tile * (kFIn / BK) + s) * kFXBytes),
+                     "r"(kFXBytes), "r"(bar)
+                     : "memory");
 }
 
 // 32 accumulator columns of this thread's row (TMEM lane) starting at column c
@@ -225,36 +223,36 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    for (int i = t; i < 3 * kFHid + kFOut; i += kFThreads)
+        sm.bias[i] = i < kFHid ? g.bias[0][i] : i < 2 * kFHid ? g.bias[1][i - kFHid]
+                   : i < 3 * kFHid ? g.bias[2][i - 2 * kFHid] : g.bias[3][i - 3 * kFHid];
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem_base;
 
-    for (int i = t; i < 3 * kFHid + kFOut; i += kFThreads)
-        sm.bias[i] = i < kFHid ? g.bias[0][i] : i < 2 * kFHid ? g.bias[1][i - kFHid]
-                   : i < 3 * kFHid ? g.bias[2][i - 2 * kFHid] : g.bias[3][i - 3 * kFHid];
-    int done_count = 0;   // completions of done_bar so far (one per layer / output pass)
-    int w_issued = 0, w_landed = 0;   // thread 0: weight tiles requested / seen complete
-    // prologue: steps 0 .. kFStages-2, one cp.async group each
-    for (int i = 0; i < kFStages - 1; ++i) {
-        if (t == 0) {
-            fused_load_w(g, sm, i);
+    // Thread 0 runs the K loop (bulk loads kFStages-1 steps ahead, MMAs, commits);
+    // all threads meet at the end of every layer / output pass for its epilogue.
+    int done_count = 0;               // completions of done_bar so far (one per layer / output pass)
+    int w_issued = 0, w_landed = 0;   // thread 0: stage fills requested / seen complete
+    if (t == 0) {
+        for (int i = 0; i < kFStages - 1; ++i) {
+            fused_load(g, sm, i, blockIdx.x);
             ++w_issued;
         }
-        fused_load_x(g, sm, i, m0);
-        asm volatile("cp.async.commit_group;" ::: "memory");
     }
     for (int s = 0; s < kFSteps; ++s) {
         const FStep f = fused_step(s);
         const int st = s % kFStages;
         if (f.kb == 0 && s > 0) {
             // the previous layer (or pass) is complete: its epilogue feeds this one
-            if (!sm.failed && !mbar_wait(smem_addr(&sm.done_bar), (uint32_t)(done_count & 1))) {
+            if (t == 0 && !sm.failed && !mbar_wait(smem_addr(&sm.done_bar), (uint32_t)(done_count & 1))) {
                 sm.failed = 1;
                 if (g.err) atomicExch(g.err, 1);
             }
             ++done_count;
             __syncthreads();
+            __syncwarp();   // tcgen05.ld is warp-collective
             const FStep p = fused_step(s - 1);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!sm.failed) {
@@ -266,83 +264,68 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
             // generic-proxy writes of the activations -> visible to the MMAs
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
         }
-        // step s has landed (at most kFStages-2 newer groups pending)
-        asm volatile("cp.async.wait_group %0;" ::"n"(kFStages - 2) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (t == 0 && !sm.failed) {
-            if (mbar_wait(smem_addr(&sm.full[st]), (uint32_t)((s / kFStages) & 1))) {
-                ++w_landed;
-            } else {
-                sm.failed = 1;
-                if (g.err) atomicExch(g.err, 1);
-            }
+        if (t != 0 || sm.failed) continue;
+        if (mbar_wait(smem_addr(&sm.full[st]), (uint32_t)((s / kFStages) & 1))) {
+            ++w_landed;
+        } else {
+            sm.failed = 1;
+            if (g.err) atomicExch(g.err, 1);
+            continue;
         }
-        if (t == 0 && !sm.failed) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int n = f.layer == 3 ? kFPass : kFHid;
-            const uint32_t idesc = instr_desc(BM, n);
-            const uint32_t a0 = smem_addr(sm.h[f.layer == 0 ? st : f.kb]);
-            const uint32_t b0 = smem_addr(sm.b[st]);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int n = f.layer == 3 ? kFPass : kFHid;
+        const uint32_t idesc = instr_desc(BM, n);
+        const uint32_t a0 = smem_addr(sm.h[f.layer == 0 ? st : f.kb]);
+        const uint32_t b0 = smem_addr(sm.b[st]);
 #pragma unroll
-            for (int k = 0; k < BK / 16; ++k) {
-                const uint64_t ad = smem_desc(a0 + k * 256, 128, 1024);
-                const uint64_t bd = smem_desc(b0 + k * 256, 128, 1024);
-                const uint32_t acc = (f.kb > 0 || k > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                    : "memory");
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_addr(&sm.bar[st]))
-                         : "memory");
-            const bool last = s + 1 == kFSteps || fused_step(s + 1).kb == 0;
-            if (last)
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_addr(&sm.done_bar))
-                             : "memory");
+        for (int k = 0; k < BK / 16; ++k) {
+            const uint64_t ad = smem_desc(a0 + k * 256, 128, 1024);
+            const uint64_t bd = smem_desc(b0 + k * 256, 128, 1024);
+            const uint32_t acc = (f.kb > 0 || k > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                : "memory");
         }
-        // prefetch step s+kFStages-1 into the stage of step s-1 once its MMAs are done
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&sm.bar[st]))
+                     : "memory");
+        const bool last = s + 1 == kFSteps || fused_step(s + 1).kb == 0;
+        if (last)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&sm.done_bar))
+                         : "memory");
+        // refill the stage of step s-1 with step s+kFStages-1 once its MMAs are done
         const int ns = s + kFStages - 1;
         if (ns < kFSteps) {
-            if (s >= 1 && !sm.failed) {
-                const uint32_t parity = (uint32_t)(((s - 1) / kFStages) & 1);
-                if (!mbar_wait(smem_addr(&sm.bar[ns % kFStages]), parity)) {
-                    sm.failed = 1;
-                    if (g.err) atomicExch(g.err, 1);
-                }
+            if (s >= 1 && !mbar_wait(smem_addr(&sm.bar[ns % kFStages]), (uint32_t)(((s - 1) / kFStages) & 1))) {
+                sm.failed = 1;
+                if (g.err) atomicExch(g.err, 1);
+                continue;
             }
-            __syncthreads();
-            if (!sm.failed) {
-                if (t == 0) {
-                    fused_load_w(g, sm, ns);
-                    ++w_issued;
-                }
-                if (ns < kFIn / BK) fused_load_x(g, sm, ns, m0);
-            }
+            fused_load(g, sm, ns, blockIdx.x);
+            ++w_issued;
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
     }
     // the last output pass
-    bool ok = !sm.failed;
-    if (ok && !mbar_wait(smem_addr(&sm.done_bar), (uint32_t)(done_count & 1))) {
-        ok = false;
+    if (t == 0 && !sm.failed && !mbar_wait(smem_addr(&sm.done_bar), (uint32_t)(done_count & 1))) {
+        sm.failed = 1;
         if (g.err) atomicExch(g.err, 1);
     }
-    ok = __all_sync(0xffffffffu, ok);   // tcgen05.ld is warp-collective
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok) fused_out_epilogue(g, sm, 1, tmem, m0);
     // no copy may still be writing this CTA's shared memory when it exits (only
-    // after a failed wait are there requested tiles that no MMA consumed)
+    // after a failed wait are there requested fills that no MMA consumed)
     if (t == 0) {
         for (int s = w_landed; s < w_issued; ++s)
             if (!mbar_wait(smem_addr(&sm.full[s % kFStages]), (uint32_t)((s / kFStages) & 1)) && g.err)
                 atomicExch(g.err, 1);
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    __syncwarp();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!sm.failed) fused_out_epilogue(g, sm, 1, tmem, m0);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
