@@ -135,6 +135,8 @@ struct FeatParams {
 template <class T, bool TILED = false>
 __global__ void __launch_bounds__(64) features_kernel(const T* __restrict__ u, FeatParams fp, bf16* __restrict__ X) {
     __shared__ float q[4][64];
+    // (tiled: the fused inference kernel that follows may start its prologue now)
+    if (TILED) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const long long e = blockIdx.x;
     const long long npts = (long long)fp.nx * fp.ny * fp.nz * 64;
     const int p = threadIdx.x, i = p & 3, j = (p >> 2) & 3, k = p >> 4;

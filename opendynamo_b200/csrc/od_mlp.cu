@@ -137,8 +137,20 @@ cudaError_t launch_fused(const FusedArgs& a, int M, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         prepared[dev] = true;
     }
-    mlp_fused_kernel<<<(unsigned)(M / BM), kFThreads, fused_smem_bytes(), s>>>(a);
-    return cudaGetLastError();
+    // programmatic dependent launch: the prologue and the first weight copies
+    // overlap the tail of the kernel before (griddepcontrol.wait in the kernel
+    // orders everything that reads its results)
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(M / BM));
+    cfg.blockDim = dim3(kFThreads);
+    cfg.dynamicSmemBytes = fused_smem_bytes();
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, mlp_fused_kernel, a);
 }
 
 }  // namespace mlp

@@ -75,8 +75,17 @@ constexpr uint32_t kFXBytes = BM * BK * 2;   // feature block of a layer-1 step
 
 // thread 0: the weight tile of step s (and for layer 1 the tile's feature
 // block) into its stage, bulk copies that complete on the stage's `full`
-// barrier
-__device__ __forceinline__ void fused_load(const FusedArgs& g, FusedSmem& sm, int s, int tile) {
+// barrier. with_x = false posts the barrier's byte count for both but copies
+// only the weights; fused_load_x then adds the features.
+__device__ __forceinline__ void fused_load_x(const FusedArgs& g, FusedSmem& sm, int s, int tile) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(sm.h[s % kFStages])),
+                 "l"(reinterpret_cast<const char*>(g.X) + ((size_t)tile * (kFIn / BK) + s) * kFXBytes), "r"(kFXBytes),
+                 "r"(smem_addr(&sm.full[s % kFStages]))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fused_load(const FusedArgs& g, FusedSmem& sm, int s, int tile, bool with_x = true) {
     const int st = s % kFStages;
     const uint32_t bar = smem_addr(&sm.full[st]);
     const uint32_t wbytes = fused_w_bytes(s);
@@ -88,12 +97,7 @@ __device__ __forceinline__ void fused_load(const FusedArgs& g, FusedSmem& sm, in
                      smem_addr(sm.b[st])),
                  "l"(reinterpret_cast<const char*>(g.Wt) + fused_w_off(s)), "r"(wbytes), "r"(bar)
                  : "memory");
-    if (feat)
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         smem_addr(sm.h[st])),
-                     "l"(reinterpret_cast<const char*>(g.X) + ((size_t)tile * (kFIn / BK) + s) * kFXBytes),
-                     "r"(kFXBytes), "r"(bar)
-                     : "memory");
+    if (feat && with_x) fused_load_x(g, sm, s, tile);
 }
 
 // 32 accumulator columns of this thread's row (TMEM lane) starting at column c
@@ -235,12 +239,18 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
     // all threads meet at the end of every layer / output pass for its epilogue.
     int done_count = 0;               // completions of done_bar so far (one per layer / output pass)
     int w_issued = 0, w_landed = 0;   // thread 0: stage fills requested / seen complete
+    // The weights and biases do not depend on the kernel launched before this
+    // one (the features, which may let this kernel start early): the first
+    // weight tiles are requested before waiting for it, the features after.
     if (t == 0) {
         for (int i = 0; i < kFStages - 1; ++i) {
-            fused_load(g, sm, i, blockIdx.x);
+            fused_load(g, sm, i, blockIdx.x, false);
             ++w_issued;
         }
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (t == 0)
+        for (int i = 0; i < kFStages - 1; ++i) fused_load_x(g, sm, i, blockIdx.x);
     for (int s = 0; s < kFSteps; ++s) {
         const FStep f = fused_step(s);
         const int st = s % kFStages;
