@@ -6,22 +6,24 @@
 // accumulator from tensor memory (tcgen05.ld), adds the bias, applies GELU,
 // rounds to bf16 and writes the result into shared memory in the canonical
 // K-major core-matrix layout the next layer's MMAs read as their A operand.
-// Only the features (layer 1's A) and the weights (every layer's B, from L2)
-// are streamed, in 64-wide K blocks, four stages deep: the weights as one
-// bulk copy per stage from a step-ordered image already in the shared-memory
-// layout (tile_fused_weights), completing on the stage's `full` mbarrier; the
-// features with 16-byte cp.async by all threads. Thread 0 issues the bulk
+// Only the features (layer 1's A, written in this kernel's tile layout by
+// the features kernel) and the weights (every layer's B, from a step-ordered
+// image in the shared-memory layout, tile_fused_weights) are streamed, in
+// 64-wide K blocks, three stages deep, as bulk copies that complete on the
+// stage's `full` mbarrier. Thread 0 alone runs the K loop: it issues the
 // copies and tcgen05.mma (kind::f16, M = 128, K = 16) and commits each stage's
-// MMAs to its `bar` mbarrier. The output layer runs as two passes of N = 160
-// (columns 0-159 and 160-319: variables 0-2.5 and 2.5-5).
+// MMAs to its `bar` mbarrier; the 16 warps meet at the end of every layer for
+// its epilogue (warp w: TMEM lanes 32 (w % 4) .. +31, column group w / 4). The
+// output layer runs as two passes of N = 160 (columns 0-159 and 160-319:
+// variables 0-2.5 and 2.5-5).
 //
-// Shared memory (209 KB): one 64 KB activation buffer of four 128 x 64
-// k-blocks, four 32 KB weight stages and a 17 KB staging area for the RHS
-// update. A layer's epilogue overwrites its own input in place: it starts
-// only after all of the layer's MMAs have completed. During layer 1 the
-// activation buffer holds the four feature stages instead (layer 1's output
-// is written after its last MMA). Tensor memory: 256 fp32 columns, reused by
-// every layer.
+// Shared memory (200 KB): one 64 KB activation buffer of four 128 x 64
+// k-blocks, three 32 KB weight stages, a 34 KB staging area for the RHS
+// update and the biases. A layer's epilogue overwrites its own input in
+// place: it starts only after all of the layer's MMAs have completed. During
+// layer 1 the activation buffer holds the feature stages instead (layer 1's
+// output is written after its last MMA). Tensor memory: 256 fp32 columns,
+// reused by every layer.
 // Every mbarrier wait is bounded: past the limit the CTA records an error,
 // skips the remaining work and frees its tensor memory.
 #pragma once
@@ -32,8 +34,9 @@ namespace od {
 namespace mlp {
 
 constexpr int kFIn = 896, kFHid = 256, kFOut = 320, kFPass = 160;
-constexpr int kFStages = 4;
-constexpr int kFThreads = 256;   // 8 warps: warp w reads TMEM lanes 32 (w % 4) .. +31, column half w / 4
+constexpr int kFStages = 3;
+constexpr int kFThreads = 512;   // 16 warps: warp w reads TMEM lanes 32 (w % 4) .. +31, column group w / 4
+constexpr int kFGroups = kFThreads / 128;   // column groups of the epilogues
 constexpr int kFSteps = kFIn / BK + 2 * (kFHid / BK) + 2 * (kFHid / BK);   // 14 + 4 + 4 + 2 x 4 = 30
 constexpr uint32_t kFStageBytes = kFHid * BK * 2;      // weight tile of a hidden-layer step
 constexpr uint32_t kFOutStageBytes = kFPass * BK * 2;  // weight tile of an output step
@@ -118,37 +121,21 @@ __device__ __forceinline__ void fused_tmem_ld32(uint32_t lane_base, int c, float
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-// 64 accumulator columns of this thread's row starting at column c, one wait
-__device__ __forceinline__ void fused_tmem_ld64(uint32_t lane_base, int c, float* v) {
-    uint32_t r[64];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(r[16 * q + 0]), "=r"(r[16 * q + 1]), "=r"(r[16 * q + 2]), "=r"(r[16 * q + 3]), "=r"(r[16 * q + 4]),
-              "=r"(r[16 * q + 5]), "=r"(r[16 * q + 6]), "=r"(r[16 * q + 7]), "=r"(r[16 * q + 8]), "=r"(r[16 * q + 9]),
-              "=r"(r[16 * q + 10]), "=r"(r[16 * q + 11]), "=r"(r[16 * q + 12]), "=r"(r[16 * q + 13]),
-              "=r"(r[16 * q + 14]), "=r"(r[16 * q + 15])
-            : "r"(lane_base + (uint32_t)(c + 16 * q)));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
-}
-
 // Epilogue of hidden layer l: bias + GELU -> bf16 rows into the activation
 // buffer (K-major tiles of 64 columns); each thread one row (its TMEM lane)
-// and one half of the columns.
+// and one column group.
 __device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedSmem& sm, int l, uint32_t tmem) {
-    const int t = threadIdx.x, warp = t >> 5, quarter = warp & 3, half = warp >> 2;
+    const int t = threadIdx.x, warp = t >> 5, quarter = warp & 3, grp = warp >> 2;
     const int row = quarter * 32 + (t & 31);
     const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
     const float* bias = sm.bias + l * kFHid;
+    constexpr int span = kFHid / kFGroups;
 #pragma unroll 1
-    for (int c0 = half * (kFHid / 2); c0 < (half + 1) * (kFHid / 2); c0 += 64) {
-        float v[64];
-        fused_tmem_ld64(lane_base, c0, v);
+    for (int c0 = grp * span; c0 < (grp + 1) * span; c0 += 32) {
+        float v[32];
+        fused_tmem_ld32(lane_base, c0, v);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < 4; ++q) {
             const float4 b0 = *reinterpret_cast<const float4*>(bias + c0 + 8 * q);
             const float4 b1 = *reinterpret_cast<const float4*>(bias + c0 + 8 * q + 4);
             const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
@@ -174,13 +161,13 @@ __device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedS
 // contiguous 64-byte row segments.
 __device__ __forceinline__ void fused_out_epilogue(const FusedArgs& g, FusedSmem& sm, int pass, uint32_t tmem,
                                                    int m0) {
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, quarter = warp & 3, half = warp >> 2;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, quarter = warp & 3, grp = warp >> 2;
     const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
     float* stg = sm.stg[warp];
     const int row0 = m0 + quarter * 32;
     const int sub = lane >> 4, col = lane & 15;
 #pragma unroll 1
-    for (int c0 = half * 32; c0 < kFPass; c0 += 64) {   // column chunks 0, 2, 4 | 1, 3
+    for (int c0 = grp * 32; c0 < kFPass; c0 += 32 * kFGroups) {   // 32-column chunks, round robin over the groups
         float v[32];
         fused_tmem_ld32(lane_base, c0, v);
         const int n = pass * kFPass + c0;   // 32 columns inside one variable's 64-point block
