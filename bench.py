@@ -120,6 +120,16 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def bench_config(world: int = 1) -> dict:
+    """The workload description both arms (ours and --impl reference) print."""
+    w = WORKLOAD
+    npts = w["nx"] * w["ny"] * w["nz"] * 64
+    return {"workload": "channel 48^3 elements, FR P=3 (7,077,888 dofs), SLAU2, y slip walls, f32",
+            "rk3_steps_per_step": RK_PER_STEP, "dt": float(np.float32(w["dt"])), "global_dofs": world * npts,
+            "l2": "inputs larger than L2 (141.6 MB state x 3 buffers > 126 MB)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
 def build_state(dtype=np.float32):
     from opendynamo_b200 import initial_state as ic
     w = WORKLOAD
@@ -244,10 +254,7 @@ def run_ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (channel IC generator: laminar profile + Fourier trip, seed 42)",
-            "config": {"workload": "channel 48^3 elements, FR P=3 (7,077,888 dofs), SLAU2, y slip walls, f32",
-                       "rk3_steps_per_step": RK_PER_STEP, "dt": dt, "global_dofs": world * npts,
-                       "l2": "inputs larger than L2 (141.6 MB state x 3 buffers > 126 MB)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": bench_config(world),
             "e2e": {"value": round(e2e_value, 3), "unit": "Gdof*stage/s",
                     "h2d_bytes_per_step": int(solver.state_bytes), "d2h_bytes_per_step": int(solver.state_bytes)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -269,13 +276,13 @@ def run_ours(args, world, rank, local):
 
 
 def run_reference(args, world, rank, local):
-    if rank != 0:
-        return None
     try:
         from oracle import ref_harness
     except Exception as exc:  # pragma: no cover
+        if rank != 0:
+            return None
         return {"impl": "reference", "unavailable": f"reference harness not importable: {exc}"}
-    return ref_harness.bench_line(args, WORKLOAD, RK_PER_STEP, METRIC, BYTES_PER_DOF_STAGE)
+    return ref_harness.bench_line(args, WORKLOAD, RK_PER_STEP, METRIC, BYTES_PER_DOF_STAGE, world, rank, local)
 
 
 def run_precision_form(args, world, rank, local):

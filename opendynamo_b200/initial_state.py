@@ -31,10 +31,43 @@ def _c(x) -> np.float32:
     return np.float32(x)
 
 
+def _legendre(p: int, x: float) -> float:
+    # src/fr_math.rs:3-21 (three-term recurrence)
+    if p == 0:
+        return 1.0
+    if p == 1:
+        return x
+    a, b, val = 1.0, x, 0.0
+    for k in range(2, p + 1):
+        val = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / float(k)
+        a, b = b, val
+    return val
+
+
+def _dlegendre(p: int, x: float) -> float:
+    # src/fr_math.rs:23-29
+    if p == 0:
+        return 0.0
+    return float(p) / (x * x - 1.0) * (x * _legendre(p, x) - _legendre(p - 1, x))
+
+
 def gauss_points() -> np.ndarray:
-    """GL points of src/fr_math.rs (the product's od_fr_tables) in double."""
-    from .solver import fr_tables
-    return fr_tables()["points"]
+    """The four Gauss-Legendre points of src/fr_math.rs:31-53 (Newton from
+    cos(pi (i + 3/4) / (n + 1/2)), step tolerance 1e-14, sorted) in double.
+    Plain Python floats, the same IEEE double operations as the library's
+    od_fr_tables, so the two agree bit for bit; computed here so that building
+    an initial state needs no CUDA library."""
+    n = 4
+    roots = []
+    for i in range(n):
+        x = math.cos(math.pi * (i + 0.75) / (n + 0.5))
+        for _ in range(100):
+            step = _legendre(n, x) / _dlegendre(n, x)
+            x -= step
+            if abs(step) < 1e-14:
+                break
+        roots.append(x)
+    return np.array(sorted(roots), dtype=np.float64)
 
 
 def _fma32(a, b, c) -> np.ndarray:

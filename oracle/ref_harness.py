@@ -153,58 +153,77 @@ class RefSolver:
         return int(self.L.refh_state_bytes(self.h))
 
 
-def bench_line(args, w, rk_per_step, metric, bytes_per_dof_stage) -> dict:
+def bench_line(args, w, rk_per_step, metric, bytes_per_dof_stage, world=1, rank=0, local=0):
     """``bench.py --impl reference``: the reference's own kernels on this GPU,
-    same workload, metric and step definition as the project's arm."""
-    import math
+    same workload, metric, config and step definition as the project's arm.
+    Under torchrun every rank runs one replica on its own GPU (as the
+    project's arm does); device time is the slowest rank's, and rank 0
+    prints the whole-job throughput. Returns None on the other ranks."""
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, root)
     import bench  # noqa: WPS433
+    from opendynamo_b200 import replicas
+    dist = None
     try:
         import torch
         torch.cuda.init()
-        local = int(os.environ.get("LOCAL_RANK", "0"))
         torch.cuda.set_device(local)
+        dist = replicas.init("nccl")
+        dev = f"cuda:{local}"
         u = bench.build_state(np.float32)
         npts = w["nx"] * w["ny"] * w["nz"] * 64
+
+        def barrier():
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+                torch.cuda.synchronize()
+
         with RefSolver(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"], w["lz"], w["flux"], w["y_wall"], "f32",
                        device=local) as r:
             r.set_state(u)
             r.time_steps(rk_per_step * args.warmup, w["dt"])
             clocks = bench.ClockSampler(local)
             clocks.start()
+            barrier()
             ms = r.time_steps(rk_per_step * args.steps, w["dt"])
+            barrier()
             clk = clocks.stop()
+            ms = replicas.max_over_ranks(ms, dist, dev)
             # e2e: state upload + 50 steps + download per bench step
+            barrier()
             t0 = time.perf_counter()
             for _ in range(args.steps):
                 r.set_state(u)
                 r.step(rk_per_step, w["dt"])
                 out = r.get_state()
-            e2e_s = time.perf_counter() - t0
+            barrier()
+            e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
             launches = r.launches_per_step * rk_per_step * args.steps
             finite = bool(np.isfinite(out).all())
         stages = args.steps * rk_per_step * 3
-        value = npts * stages / (ms / 1e3) / 1e9
-        e2e = npts * stages / e2e_s / 1e9
-        return {
+        value = replicas.job_throughput(npts * stages, ms / 1e3, world) / 1e9
+        e2e = replicas.job_throughput(npts * stages, e2e_s, world) / 1e9
+        line = {
             "impl": "reference", "metric": metric, "value": round(value, 3), "unit": "Gdof*stage/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (channel IC generator: laminar profile + Fourier trip, seed 42)",
-            "config": {"workload": "channel 48^3 elements, FR P=3 (7,077,888 dofs), SLAU2, y slip walls, f32",
-                       "rk3_steps_per_step": rk_per_step, "dt": float(np.float32(w["dt"])),
-                       "implementation": "reference CUDA sources, NVRTC compute_100 --use_fast_math, "
-                                         "driver JIT, solver.rs launch shapes and sequence",
-                       "l2": "inputs larger than L2"},
+            "config": bench.bench_config(world),
+            "implementation": "the reference's CUDA sources (constants.cuh, device_functions.cuh, rhs.cu, rk.cu), "
+                              "NVRTC compute_100 --use_fast_math, driver JIT, src/solver.rs launch shapes and "
+                              "sequence; it has no CPU path",
             "e2e": {"value": round(e2e, 3), "unit": "Gdof*stage/s", "h2d_bytes_per_step": int(u.nbytes),
                     "d2h_bytes_per_step": int(u.nbytes)},
-            "cpu_baseline": {"value": round(value, 3), "unit": "Gdof*stage/s", "cores": 0, "kind": "reference",
-                             "sample": "the reference has no CPU path: its own CUDA kernels on this GPU, "
-                                       f"{args.steps} x {rk_per_step} RK3 steps"},
             "gpu_launches": launches, "clocks": clk, "state_finite": finite,
         }
+        replicas.finish(dist)
+        return line if rank == 0 else None
     except Exception as exc:
+        if dist is not None:
+            replicas.finish(dist)
+        if rank != 0:
+            return None
         return {"impl": "reference", "unavailable": f"reference kernels could not run: {exc}"}

@@ -27,6 +27,31 @@ def test_gauss_points_match_script():
     assert np.array_equal(d["gl_points"], fr_tables()["points"])
 
 
+def test_ic_gauss_points_match_library_bit_for_bit():
+    """The IC module computes the GL points itself (no CUDA library needed to
+    build a state); they must equal od_fr_tables' points exactly."""
+    a = ic.gauss_points()
+    b = fr_tables()["points"]
+    assert a.dtype == np.float64
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), (a, b)
+
+
+def test_ic_module_does_not_load_the_library():
+    """Building the bench's initial state must not load libopendynamo.so (the
+    reference arm builds its state with this module)."""
+    import subprocess
+    import sys
+    code = ("import sys, numpy as np; sys.path.insert(0, %r)\n"
+            "from opendynamo_b200 import initial_state as ic\n"
+            "ic.stack(ic.channel_state(4, 3, 2, 6.283185307179586, 2.0, 3.141592653589793, 0.2, 'channel', 0.01,"
+            " 16, 42), np.float32)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libopendynamo' not in maps, 'library loaded'\n") % os.path.dirname(os.path.dirname(
+                os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 @pytest.mark.parametrize("n", range(4))
 def test_channel_ic_bit_exact(n):
     d, cases = _cases()
