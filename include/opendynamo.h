@@ -82,6 +82,15 @@ enum { OD_COMPAT_Y_SLICE_F32 = 1 };
 /* Reference defaults: SLAU2, slip walls, all f32, mu 1.6e-4 constant, forcing 1e-3. */
 void od_default_params(od_params* p);
 
+/* Layout checks for hosts that declare od_params themselves (a Rust
+ * #[repr(C)] struct, ctypes): sizeof(od_params) as compiled into the
+ * library, and the ABI version, raised whenever a struct of this header
+ * changes its fields. No counterpart in the reference (its host and kernels
+ * are compiled together, src/solver.rs:380-447). */
+#define OD_ABI_VERSION 2
+size_t od_params_size(void);
+int od_abi_version(void);
+
 /* Allocate device buffers and prepare the kernels.
  * Replaces: run_solver_generic setup — compile_module / load_kernels /
  * setup_fr_operators / allocate_buffers (src/solver.rs:147-159, 432-601). */
@@ -213,7 +222,12 @@ int od_timing(od_ctx* ctx, double* ms_phase_a, double* ms_phase_b, long long* n_
  * OD_ERR_SCRATCH. All calls share the array: calls whose kernels overlap on
  * the GPU race, so order them on one stream. The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) and sets the kernels'
- * shared-memory limits; make it before any stream capture. Runs on
+ * shared-memory limits; make it before any stream capture. With CUDA's lazy
+ * module loading that first call (per device and precision combination) is
+ * also where the driver loads the kernels and places the array in device
+ * memory, so it can take device memory: make it during initialisation,
+ * outside any window in which allocation is forbidden; later calls allocate
+ * nothing. Runs on
  * params->device (the caller's current device is restored) and enqueues on
  * `stream` (cudaStream_t, null = legacy default stream); returns before the
  * kernels finish. */
@@ -382,6 +396,18 @@ int od_ensemble_get_state(od_ensemble* e, int box, void* host, size_t bytes);
 /* n SSP-RK3 steps of every box; waits for completion and reports a timed-out
  * grid barrier (the bounded wait's error flag) as OD_ERR_CUDA. */
 int od_ensemble_step(od_ensemble* e, int n_steps);
+/* The grid barrier's bounded wait: a block polls the arrival counter at most
+ * spin_limit times (about 100 ns apart; 0 = the default 2^25, seconds) and
+ * then sets the error flag and returns, skipping the rest of the stage;
+ * od_ensemble_step then returns OD_ERR_CUDA and the states are undefined
+ * until set again. extra_arrivals > 0 raises every barrier target by that
+ * many arrivals, which no launch reaches: a wait that must run out, for
+ * testing the error path without faulting or hanging the GPU. The call
+ * also restarts the arrival counter and clears the error flag, so it is how
+ * a host recovers after a timed-out barrier (od_ensemble_set_wait(e, 0, 0)).
+ * No reference counterpart. */
+int od_ensemble_set_wait(od_ensemble* e, long long spin_limit, int extra_arrivals);
+
 /* Launch shape: elements per block (2 or 4; 16 threads each), blocks per SM
  * (<= 0: all that are co-resident), CUDA graph on/off. */
 int od_ensemble_set_shape(od_ensemble* e, int elems_per_block, int blocks_per_sm, int use_graph);
@@ -399,6 +425,14 @@ void* od_ensemble_stream(od_ensemble* e);
  * K % 64 == 0. Synchronous on `stream`. Exposed for tests; the closure uses
  * the same kernel with fused epilogues. No reference counterpart. */
 int od_gemm_bf16(int M, int N, int K, const void* dA, const void* dB, float* dC, const float* dbias, void* stream);
+
+/* Self-test of the bounded mbarrier wait that every tcgen05 kernel of the
+ * closure uses (copies and MMAs signal mbarriers; a wait gives up after a
+ * poll limit, sets the kernel's error flag and returns). One block on
+ * `device`: a wait on a barrier nothing arrives on, with `limit` polls, must
+ * give up (*first_completed = 0); after one arrival the same wait must
+ * complete (*second_completed = 1). Synchronous. No reference counterpart. */
+int od_mlp_wait_selftest(long long limit, int device, int* first_completed, int* second_completed);
 
 /* ------------------------------------------------------------------------
  * Learned closure (no reference counterpart): a per-element MLP

@@ -20,15 +20,15 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "size mismatch", -4: "ca
 
 # every symbol include/opendynamo.h declares
 EXPORTS = (
-    "od_default_params", "od_create", "od_destroy", "od_state_bytes", "od_set_state", "od_get_state",
+    "od_default_params", "od_params_size", "od_abi_version", "od_create", "od_destroy", "od_state_bytes", "od_set_state", "od_get_state",
     "od_set_state_device", "od_get_state_device", "od_step", "od_rhs", "od_sync", "od_stream",
     "od_launches_per_step", "od_set_launch_shape", "od_set_pipeline_slabs", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
     "od_rhs_noalloc", "od_state_save", "od_state_info", "od_state_load", "od_state_error", "od_run",
     "od_diagnostics",
     "od_ensemble_create", "od_ensemble_destroy", "od_ensemble_state_bytes", "od_ensemble_set_state",
-    "od_ensemble_get_state", "od_ensemble_step", "od_ensemble_set_shape", "od_ensemble_info",
+    "od_ensemble_get_state", "od_ensemble_step", "od_ensemble_set_wait", "od_ensemble_set_shape", "od_ensemble_info",
     "od_ensemble_autotune", "od_ensemble_last_error", "od_ensemble_stream",
-    "od_gemm_bf16",
+    "od_gemm_bf16", "od_mlp_wait_selftest",
     "od_mlp_create", "od_mlp_destroy", "od_mlp_last_error", "od_mlp_param_count", "od_mlp_set_params",
     "od_mlp_get_params", "od_mlp_forward", "od_mlp_gradients", "od_mlp_train_step", "od_mlp_set_scaling",
     "od_mlp_set_fused",
@@ -100,6 +100,8 @@ def lib() -> ctypes.CDLL:
     P = ctypes.POINTER(OdParams)
     sig = {
         "od_default_params": (None, [P]),
+        "od_params_size": (ctypes.c_size_t, []),
+        "od_abi_version": (ci, []),
         "od_create": (ci, [P, ctypes.POINTER(vp)]),
         "od_destroy": (None, [vp]),
         "od_state_bytes": (sz, [vp]),
@@ -135,6 +137,8 @@ def lib() -> ctypes.CDLL:
         "od_ensemble_set_state": (ci, [vp, ci, vp, sz]),
         "od_ensemble_get_state": (ci, [vp, ci, vp, sz]),
         "od_ensemble_step": (ci, [vp, ci]),
+        "od_ensemble_set_wait": (ci, [vp, ctypes.c_longlong, ci]),
+        "od_mlp_wait_selftest": (ci, [ctypes.c_longlong, ci, ctypes.POINTER(ci), ctypes.POINTER(ci)]),
         "od_ensemble_set_shape": (ci, [vp, ci, ci, ci]),
         "od_ensemble_info": (ci, [vp, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci),
                                   ctypes.POINTER(ci)]),

@@ -362,6 +362,10 @@ void od_default_params(od_params* p) {
     p->s_suth = 110.4;
 }
 
+size_t od_params_size(void) { return sizeof(od_params); }
+
+int od_abi_version(void) { return OD_ABI_VERSION; }
+
 int od_fr_tables(double* out) {
     if (!out) return OD_ERR_ARG;
     od::TablesD t = build_tables();
@@ -455,7 +459,7 @@ int od_create(const od_params* p, od_ctx** out) {
             return cuda_fail(c, e, "cudaMalloc RHS buffer");
         }
     }
-    // viscous face fluxes [elem][6][4][16] + minus-face interface fluxes [elem][3][5][16]
+    // plus-face viscous fluxes [elem][3][4][16] + minus-face records F_I - 1/2 Fv [elem][3][5][16]
     const size_t fv_bytes = (size_t)nelem * od::kFaceWords * (c->fns.c_double ? 8 : 4);
     e = cudaMalloc(&c->fv, fv_bytes);
     if (e != cudaSuccess) {

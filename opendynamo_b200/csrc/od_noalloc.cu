@@ -23,6 +23,12 @@
 // host-side stand-in, not a device address). The first call on each device
 // looks up the device address with cudaGetSymbolAddress, with that device
 // current, and caches it; make that first call before any stream capture.
+// With CUDA's lazy module loading (the default since CUDA 12.2) that first
+// call is also where the driver loads this library's kernels and
+// materialises the array on the device, which does take device memory: make
+// the first call for each device and precision combination during
+// initialisation, outside any window in which allocation is forbidden.
+// Every later call allocates nothing.
 
 #include <mutex>
 
@@ -66,8 +72,8 @@ extern "C" int od_rhs_noalloc(const od_params* p, const void* d_state, void* d_r
     const long long nelem = (long long)p->nx * p->ny * p->nz;
     if ((size_t)nelem * 64 * 5 * (s_double ? 8 : 4) != bytes) return OD_ERR_SIZE;
     if (d_state == d_rhs) return OD_ERR_ARG;
-    // viscous face fluxes (6 faces x 4 components) and minus-face interface
-    // fluxes (3 faces x 5 components), 16 points each, per element
+    // plus-face viscous fluxes (3 faces x 4 components) and minus-face
+    // records F_I - 1/2 Fv (3 faces x 5 components), 16 points each, per element
     const size_t scratch = (size_t)nelem * od::kFaceWords * (c_double ? 8 : 4);
     if (scratch > (size_t)OD_NOALLOC_SCRATCH_BYTES) return OD_ERR_SCRATCH;
 
@@ -136,7 +142,7 @@ extern "C" int od_rhs_noalloc(const od_params* p, const void* d_state, void* d_r
     L.flags = flags;
     L.flux = p->flux;
     L.epb_a = 4;
-    L.epb_b = 16;
+    L.epb_b = 2;   // the phase-B kernel od_rhs runs (a thread per element, variable and x-line)
     L.phases = 3;
     L.e0 = 0;
     L.e1 = nelem;

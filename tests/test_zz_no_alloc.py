@@ -23,6 +23,18 @@ from opendynamo_b200.solver import Solver, make_params
 BOX = (2 * math.pi, 2.0, math.pi)
 RHS_TOL = {"f64": 1e-11, "f32": 5e-5}
 
+# (stored type, extra make_params keywords, flux, slip walls): every precision
+# combination the library compiles, Sutherland's law and a periodic y
+CASES = {
+    "f32": ("f32", {}, "slau2", True),
+    "f64": ("f64", {}, "ausm+", True),
+    "u64c32": ("f64", {"q_real": "f32", "rhs_real": "f32", "compute_real": "f32"}, "slau2", True),
+    "u32c64": ("f32", {"q_real": "f64", "rhs_real": "f64", "compute_real": "f64"}, "rusanov", True),
+    "mixed": ("f64", {"mixed": True}, "slau2", True),
+    "f32_sutherland": ("f32", {"viscosity_model": "sutherland", "mu": 0.2 / 3000}, "slau2", True),
+    "f32_periodic": ("f32", {}, "rusanov", False),
+}
+
 
 def _noalloc(params, d_state, d_out):
     return N.lib().od_rhs_noalloc(ctypes.byref(params), ctypes.c_void_p(d_state.data_ptr()),
@@ -30,19 +42,21 @@ def _noalloc(params, d_state, d_out):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["f32", "f64"])
-def test_rhs_noalloc_matches_od_rhs_twice(prec):
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_rhs_noalloc_matches_od_rhs_twice(case):
     import torch
+    u_real, kw, flux, wall = CASES[case]
     mesh = (4, 3, 5)
-    dtype = np.float64 if prec == "f64" else np.float32
+    dtype = np.float64 if u_real == "f64" else np.float32
     states = [channel_trip(*mesh, amp=0.02, dtype=dtype), random_smooth(*mesh, seed=5, dtype=dtype)]
-    params = make_params(*mesh, *BOX, "slau2", True, prec)
+    params = make_params(*mesh, *BOX, flux, wall, u_real, **kw)
+    tol = RHS_TOL["f64" if params.compute_real == N.OD_F64 and not params.mixed else "f32"]
     refs = []
     for u in states:
         with Solver(params) as s:
             s.set_state(u)
             refs.append(s.rhs())
-    tdt = torch.float64 if prec == "f64" else torch.float32
+    tdt = torch.float64 if u_real == "f64" else torch.float32
     d_state = torch.empty(states[0].size, dtype=tdt, device="cuda:0")
     d_out = torch.empty_like(d_state)
     torch.cuda.synchronize()
@@ -55,7 +69,7 @@ def test_rhs_noalloc_matches_od_rhs_twice(prec):
         torch.cuda.synchronize()
         got = d_out.cpu().numpy()
         err = rel_l2(got, ref)
-        assert np.all(err < RHS_TOL[prec]), (call, err)
+        assert np.all(err < tol), (call, err)
         free = torch.cuda.mem_get_info(0)[0]
         if free_after_first is None:
             free_after_first = free
