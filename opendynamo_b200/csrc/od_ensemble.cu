@@ -113,10 +113,15 @@ struct StageB {
     long long e0, e1;
 };
 
+// Grid-barrier state in device memory. spin_limit and extra_arrivals are
+// set by od_ensemble_set_wait (0 = defaults): the polls a block makes before
+// it gives up, and arrivals added to the barrier target (a target nothing
+// reaches makes every wait run out: the error path's test).
 struct GridSync {
     unsigned long long count;
     int err;
-    int pad;
+    int extra_arrivals;
+    long long spin_limit;
 };
 
 constexpr long long kSpinLimit = 1LL << 25;
@@ -146,12 +151,13 @@ __device__ __forceinline__ bool grid_barrier(GridSync* g) {
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned long long n = gridDim.x;
+        const long long limit = g->spin_limit > 0 ? g->spin_limit : kSpinLimit;
         const unsigned long long old = atomicAdd(&g->count, 1ull);
-        const unsigned long long target = (old / n + 1) * n;
+        const unsigned long long target = (old / n + 1) * n + (unsigned long long)max(g->extra_arrivals, 0);
         int good = 1;
         for (long long it = 0;; ++it) {
             if (ld_acquire(&g->count) >= target) break;
-            if (it >= kSpinLimit || *(volatile int*)&g->err) {
+            if (it >= limit || *(volatile int*)&g->err) {
                 atomicExch(&g->err, 1);
                 good = 0;
                 break;
@@ -588,6 +594,19 @@ int od_ensemble_step(od_ensemble* E, int n) {
     cudaSetDevice(E->device);
     if (int rc = enqueue_steps(E, n)) return rc;
     return check_sync_flag(E);
+}
+
+int od_ensemble_set_wait(od_ensemble* E, long long spin_limit, int extra_arrivals) {
+    if (!E || spin_limit < 0 || extra_arrivals < 0) return OD_ERR_ARG;
+    cudaSetDevice(E->device);
+    GridSync h{};
+    h.spin_limit = spin_limit;
+    h.extra_arrivals = extra_arrivals;
+    // restarts the arrival counter and clears a timed-out barrier's error flag
+    cudaError_t c = cudaMemcpyAsync(E->d_sync, &h, sizeof h, cudaMemcpyHostToDevice, E->stream);
+    if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
+    if (c != cudaSuccess) return ecuda(E, c, "od_ensemble_set_wait");
+    return OD_OK;
 }
 
 int od_ensemble_set_shape(od_ensemble* E, int epb, int blocks_per_sm, int use_graph) {

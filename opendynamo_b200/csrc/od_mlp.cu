@@ -153,8 +153,45 @@ cudaError_t launch_fused(const FusedArgs& a, int M, cudaStream_t s) {
     return cudaLaunchKernelEx(&cfg, mlp_fused_kernel, a);
 }
 
+// Self-test of the bounded mbarrier wait of the tcgen05 kernels: a barrier
+// nothing arrives on must give up after `limit` polls; after one arrival the
+// same wait completes. out[0] = first wait completed, out[1] = second.
+__global__ void mbar_wait_selftest_kernel(long long limit, int* out) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0) return;
+    const uint32_t b = smem_addr(&bar);
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const bool first = mbar_wait(b, 0, limit);
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(b) : "memory");
+    const bool second = mbar_wait(b, 0, limit);
+    out[0] = first ? 1 : 0;
+    out[1] = second ? 1 : 0;
+}
+
 }  // namespace mlp
 }  // namespace od
+
+extern "C" int od_mlp_wait_selftest(long long limit, int device, int* first_completed, int* second_completed) {
+    if (limit <= 0 || !first_completed || !second_completed) return OD_ERR_ARG;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return OD_ERR_CUDA;
+    int* d = nullptr;
+    int h[2] = {-1, -1};
+    cudaError_t e = cudaMalloc((void**)&d, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d, 0xff, 2 * sizeof(int));
+    if (e == cudaSuccess) {
+        od::mlp::mbar_wait_selftest_kernel<<<1, 32>>>(limit, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return OD_ERR_CUDA;
+    *first_completed = h[0];
+    *second_completed = h[1];
+    return OD_OK;
+}
 
 extern "C" int od_gemm_bf16(int M, int N, int K, const void* dA, const void* dB, float* dC, const float* dbias,
                             void* stream) {

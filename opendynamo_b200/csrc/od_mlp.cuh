@@ -112,8 +112,11 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (long long it = 0; it < kWaitLimit; ++it) {
+// Bounded wait for the given phase parity: false after `limit` polls (the
+// caller then sets its error flag, waits for its own copies with the same
+// bound, frees its tensor memory and returns).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = kWaitLimit) {
+    for (long long it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"

@@ -131,6 +131,13 @@ class Ensemble:
     def step(self, n: int = 1):
         self._chk(self._lib.od_ensemble_step(self._h, int(n)), "od_ensemble_step")
 
+    def set_wait(self, spin_limit: int = 0, extra_arrivals: int = 0):
+        """Grid-barrier wait limit (0 = default) and extra arrivals (> 0: a
+        target no launch reaches, the timeout path); also clears a timed-out
+        barrier's error flag."""
+        self._chk(self._lib.od_ensemble_set_wait(self._h, int(spin_limit), int(extra_arrivals)),
+                  "od_ensemble_set_wait")
+
     def set_shape(self, elems_per_block: int, blocks_per_sm: int = 0, graph: bool = True):
         self._chk(self._lib.od_ensemble_set_shape(self._h, elems_per_block, blocks_per_sm, int(graph)),
                   "od_ensemble_set_shape")

@@ -115,3 +115,35 @@ def test_benchmark_boxes_are_seeded():
     mach = np.array([x.mach for x in a])
     assert mach.min() >= 0.05 and mach.max() <= 0.3
     assert {x.flux for x in a} == {"rusanov", "slau2"} and {x.kind for x in a} == {"tgv", "channel"}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph", [True, False])
+def test_barrier_timeout_is_reported_and_recoverable(graph):
+    """The grid barrier's bounded wait: with a target one arrival above the
+    grid (nothing ever reaches it) and a short poll limit, every block gives
+    up, sets the error flag and returns; od_ensemble_step reports
+    OD_ERR_CUDA with the barrier message; after od_ensemble_set_wait(0, 0)
+    the same ensemble steps correctly again."""
+    import time
+    from opendynamo_b200 import _native as N
+    states = _states(BOXES)
+    want = _alone(BOXES, states, 2)
+    with Ensemble(BOXES) as E:
+        E.set_shape(4, 0, graph)
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.set_wait(spin_limit=20000, extra_arrivals=1)
+        t0 = time.perf_counter()
+        with pytest.raises(N.OdError, match="grid barrier timed out"):
+            E.step(2)
+        assert time.perf_counter() - t0 < 30.0   # bounded: about 3 x 20000 polls of ~100 ns
+        # the flag is sticky until cleared
+        with pytest.raises(N.OdError, match="grid barrier timed out"):
+            E.step(1)
+        E.set_wait(0, 0)
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.step(2)
+        for k in range(len(BOXES)):
+            _close(E.get_state(k), want[k])

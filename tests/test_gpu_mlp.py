@@ -41,3 +41,18 @@ def test_gemm_rejects_bad_shapes():
                                 None) == -1
     assert N.lib().od_gemm_bf16(128, 100, 64, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_void_p(1), None,
                                 None) == -1
+
+
+@pytest.mark.gpu
+def test_bounded_mbarrier_wait_gives_up_and_completes():
+    """The tcgen05 kernels' bounded mbarrier wait: on a barrier nothing
+    arrives on it returns false after the poll limit (no hang, no fault); the
+    same barrier after one arrival completes."""
+    import ctypes
+    import time
+    from opendynamo_b200 import _native as N
+    a, b = ctypes.c_int(-1), ctypes.c_int(-1)
+    t0 = time.perf_counter()
+    assert N.lib().od_mlp_wait_selftest(10000, 0, ctypes.byref(a), ctypes.byref(b)) == 0
+    assert time.perf_counter() - t0 < 30.0
+    assert a.value == 0 and b.value == 1
