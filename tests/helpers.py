@@ -46,18 +46,40 @@ def tgv(n, dtype=np.float64) -> np.ndarray:
     return ic.stack(ic.taylor_green_state(n), dtype)
 
 
-def assert_f32_parity(got, ref, truth, bar=1e-5, slack=2.0, floor=1e-6):
-    """f32 parity between two f32 implementations (got, ref) of the same run.
+def ulp_perturbed(u: np.ndarray, seed: int = 1, ulp_of=np.float32) -> np.ndarray:
+    """u with every value moved by -1, 0 or +1 ulp (seeded): the smallest
+    change a different but equally exact implementation makes. The ulp is
+    that of ``ulp_of``, the arithmetic that rounds (f32 for the f32 and the
+    f32-compute pipelines, also when the stored state is f64)."""
+    rng = np.random.default_rng(seed)
+    s = rng.integers(-1, 2, size=u.size).astype(u.dtype)
+    step = np.abs(np.spacing(u.astype(ulp_of))).astype(u.dtype)
+    return (u + s * step).astype(u.dtype)
 
-    rho, rho*u and E (O(1) planes) must agree within ``bar`` relative L2.
-    rho*v and rho*w are O(1e-2) planes whose f32 round-off (absolute ~1e-7
-    from the pressure gradient) is already ~1e-5..1e-4 *relative*; for every
-    plane ``got`` must be no further from the f64 solution ``truth`` than
-    ``slack`` times the reference's own distance (or ``floor``)."""
+
+def assert_f32_parity(got, ref, truth, spread, bar=1e-5, k=2.0, slack=2.0, floor=1e-6):
+    """f32 parity between two f32 implementations (got, ref) of the same run,
+    per variable, against a measured floor.
+
+    ``spread`` is the reference's own reproducibility floor for this run: its
+    relative L2 distance, per variable, to itself started from the same state
+    moved by one f32 ulp (``ulp_perturbed``). ``truth`` is the f64 solution.
+    Two f32 implementations whose roundings are independent differ by about
+    sqrt(2) times their own f32 error once the flow has amplified round-off,
+    so every variable must satisfy
+
+        rel_l2(got, ref) < max(bar, k * spread, sqrt(2) * rel_l2(ref, truth))
+
+    i.e. ours agrees with the reference within 1e-5, or within twice the
+    reference's one-ulp spread, or within what two independent f32 roundings
+    of the reference's own accuracy give; and ``got`` must be no further from
+    the f64 solution than ``slack`` times the reference's own distance (or
+    ``floor``)."""
     e_pair = rel_l2(got, ref)
     e_got = rel_l2(got, truth)
     e_ref = rel_l2(ref, truth)
-    big = [0, 1, 4]
-    assert np.all(e_pair[big] < bar), ("O(1) planes differ", e_pair)
+    spread = np.asarray(spread, dtype=np.float64)
+    lim = np.maximum(np.maximum(bar, k * spread), math.sqrt(2.0) * e_ref)
+    assert np.all(e_pair < lim), ("f32 pair error above its floor", e_pair, spread, e_ref)
     assert np.all(e_got <= np.maximum(slack * e_ref, floor)), ("less accurate than the reference in f32", e_got, e_ref)
     return e_pair, e_got, e_ref
