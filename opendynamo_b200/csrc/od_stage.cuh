@@ -22,8 +22,9 @@
 //        F_I - 1/2 Fv_own at the minus faces (all the minus neighbour still
 //        needs at its plus face), Fv_own at the plus faces
 //   P6  x-threads: pointwise Euler - viscous fluxes of their 4 points
-//        (rhs.cu:229-266) -> smem
-//   P7  divergence along x, y, z lines
+//        (rhs.cu:229-266); F_y, F_z -> smem, the x-divergence of the
+//        thread's own x-line accumulated in registers
+//   P7  divergence along y and z lines
 //   P8  x-threads: RHS = -div + forcing (rhs.cu:505-509), lifting
 //        -(j_L g_L' + j_R g_R') jac (rk.cu:12-25), RK combination
 //        a*u0 + b*u + c*(RHS + lift) (rk.cu:27-83), 128-bit stores.
@@ -177,6 +178,24 @@ __device__ __forceinline__ void deriv4(const T* q, const DM& D, T* r) {
     }
 }
 
+// Sum over the four lanes of an aligned lane group (4g .. 4g+3) of p[q], for
+// lane q = lane & 3 of the group: a reduce-scatter in two shuffle rounds
+// (partner lane ^ 2 for the pair of components a lane keeps, then lane ^ 1).
+// Every lane forms (p_q + p_q^2) + (p_q^1 + p_q^3), which by commutativity is
+// the same value, (p_0 + p_2) + (p_1 + p_3), for all four. All 32 lanes of
+// the warp must call it together.
+template <class T>
+__device__ __forceinline__ T sum4_scatter(const T (&p)[4], int q) {
+    const bool hi = (q & 2) != 0;
+    const T a0 = hi ? p[2] : p[0], a1 = hi ? p[3] : p[1];
+    const T b0 = hi ? p[0] : p[2], b1 = hi ? p[1] : p[3];
+    const T c0 = a0 + __shfl_xor_sync(0xffffffffu, b0, 2);
+    const T c1 = a1 + __shfl_xor_sync(0xffffffffu, b1, 2);
+    const bool odd = (q & 1) != 0;
+    const T d = odd ? c1 : c0, e = odd ? c0 : c1;
+    return d + __shfl_xor_sync(0xffffffffu, e, 1);
+}
+
 // neighbour across face (d, side) or -1 for a slip wall
 __device__ __forceinline__ long long neighbour(const Mesh& m, int ex, int ey, int ez, int d, int side) {
     int c0 = ex, c1 = ey, c2 = ez;
@@ -279,7 +298,7 @@ struct SlotBytes {
 // Shared-memory slot of one element in phase A.
 template <class P, class C>
 struct alignas(16) SlotA {
-    C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9, F_x rows 10-14; P7: div_z / div_x in place
+    C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9; P7: div_z in place
     P u[NV][NE];          // state; P7: div_y (as C)
     C j[4][NV][NF];       // y / z face corrections without -1/2 Fv_nbr [face - 2][var][face pt]; the x faces of
                           // a line belong to its own thread and stay in registers
@@ -403,15 +422,52 @@ __device__ __forceinline__ void row_line_store(T* row, const LineIdx& li, const 
 }
 
 // P2-P4: one direction of the gradient / face-value pass for line l.
+// qx: the thread's own x-line as P1 loaded it (used by the x pass instead of
+// reading it back from shared memory).
 template <class M, int FLUX, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
-__device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, const LineIdx& li, const long long nb0,
-                                          const long long nb1, P* oL, P* oR, C (&jx)[2][NV], C* fi) {
+__device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, long long e, int l, const LineIdx& li,
+                                          bool live, const long long nb0, const long long nb1, P* oL, P* oR,
+                                          C (&jx)[2][NV], C* fi, const P (&qx)[NV][4]) {
     using S = typename PA::S_t;
     const Mesh& m = A.m;
     P q[NV][4];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) row_line_load<D>(sm.u[v], li, q[v]);
+    for (int v = 0; v < NV; ++v) {
+        if constexpr (D == 0) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) q[v][a] = qx[v][a];
+        } else {
+            row_line_load<D>(sm.u[v], li, q[v]);
+        }
+    }
     P nL[NV], nR[NV];
+    if constexpr (D == 1) {
+        // y neighbours: the neighbour's x-line l (points (0..3, j, k), j = l & 3,
+        // k = l >> 2) in one 128-bit load per variable, weighted with the trace
+        // coefficient of row j and summed over the four rows of the k-plane by
+        // the four lanes that hold them, so that lane l ends with the trace at
+        // face point (i, k) = (l & 3, l >> 2), its own y-line. Slip walls (no
+        // neighbour) load nothing and mirror the own face value instead.
+        const int q4 = l & 3;
+        const P cm = A.tp.eR[q4], cp = A.tp.eL[q4];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            trace4_lr(q[v], A.tp.eL, A.tp.eR, oL[v], oR[v]);
+            const P refl = (v > 0 && v < 4) ? (P)-1.0 : (P)1.0;
+            P wm[4] = {(P)0, (P)0, (P)0, (P)0}, wp[4] = {(P)0, (P)0, (P)0, (P)0};
+            if (nb0 >= 0) ldg4<S, P>(A.u_in + v * m.npts + nb0 * NE + 4 * l, wm);
+            if (nb1 >= 0) ldg4<S, P>(A.u_in + v * m.npts + nb1 * NE + 4 * l, wp);
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                wm[a] *= cm;
+                wp[a] *= cp;
+            }
+            const P sL = sum4_scatter(wm, q4);
+            const P sR = sum4_scatter(wp, q4);
+            nL[v] = nb0 >= 0 ? sL : oL[v] * refl;
+            nR[v] = nb1 >= 0 ? sR : oR[v] * refl;
+        }
+    } else {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         trace4_lr(q[v], A.tp.eL, A.tp.eR, oL[v], oR[v]);
@@ -442,6 +498,7 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, c
         } else {
             nR[v] = oR[v] * refl;
         }
+    }
     }
     // corrected gradient along the line (BR1): jl g_L' + jr g_R' + D q, all
     // scaled by the Jacobian, as one FMA chain per point
@@ -483,9 +540,10 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, int l, c
 // the neighbour's phase B: F_I - 1/2 Fv_own at a minus face (fi: the
 // interface flux solved in the line pass), Fv_own (components 1..4) at a
 // plus face.
-template <class M, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
+// REG: the face's correction j is in registers (jreg), else in shared memory.
+template <class M, int D, bool REG, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long long e, int l, int side,
-                                             const P* qp, const C* gt, bool live, C (&jx)[2][NV], const C* fi) {
+                                             const P* qp, const C* gt, bool live, C* jreg, const C* fi) {
     const int f = 2 * D + side;
     C praw;
     FaceState<C> s = make_face_state<M, C, P>(qp, praw);
@@ -493,8 +551,8 @@ __device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long 
     viscous_flux<D>(s, praw, gt, viscosity<M>(A.mu, A.suth, s), fv);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        if constexpr (D == 0)
-            jx[side][v] += (C)0.5 * fv[v];
+        if constexpr (REG)
+            jreg[v] += (C)0.5 * fv[v];
         else
             sm.j[f - 2][v][l] += (C)0.5 * fv[v];
     }
@@ -559,8 +617,8 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
             trace4_lr(w, A.tp.eL, A.tp.eR, qL[v], qR[v]);
         }
     }
-    if (!wall0) viscous_face<M, D>(A, sm, e, l, 0, qL, gL, live, jx, fi);
-    if (!wall1) viscous_face<M, D>(A, sm, e, l, 1, qR, gR, live, jx, fi);
+    if (!wall0) viscous_face<M, D, D == 0>(A, sm, e, l, 0, qL, gL, live, jx[0], fi);
+    if (!wall1) viscous_face<M, D, D == 0>(A, sm, e, l, 1, qR, gR, live, jx[1], fi);
 }
 
 // P7: divergence of F_D along the line of thread l (Dm: the Jacobian-scaled
@@ -582,7 +640,7 @@ __device__ __forceinline__ void div_pass(const C* F, C* out, const LineIdx& li, 
 // unrounded RHS + own lift for phase B.
 template <class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, long long ec, int l, int swz,
-                                               const C* divy, const C (&jx)[2][NV]) {
+                                               const C (&divx)[NV][4], const C* divy, const C (&jx)[2][NV]) {
     using S = typename PA::S_t;
     const Mesh& m = A.m;
     const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
@@ -590,8 +648,8 @@ __device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, lon
     const bool defer = (A.flags & kDeferRK) != 0;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        C dx[4], dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
-        ld4s(&sm.g[10 + v][px], dx);
+        C dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
+        const C* dx = divx[v];
         ld4s(&divy[v * NE + px], dy);
         ld4s(&sm.g[5 + v][px], dz);
         ld4s(&sm.j[0][v][4 * lk], jy0);
@@ -655,17 +713,17 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     const long long nym = neighbour(m, ex, ey, ez, 1, 0), nyp = neighbour(m, ex, ey, ez, 1, 1);
     const long long nzm = neighbour(m, ex, ey, ez, 2, 0), nzp = neighbour(m, ex, ey, ez, 2, 1);
 
-    // ---- P1: the element's x-lines -> smem
+    // ---- P1: the element's x-lines -> smem (and kept for the x pass)
+    P qx[NV][4];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        P w[4];
         if (live) {
-            ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, w);
+            ldg4<S, P>(A.u_in + v * m.npts + ec * NE + 4 * l, qx[v]);
         } else {
 #pragma unroll
-            for (int a = 0; a < 4; ++a) w[a] = (P)1.0;
+            for (int a = 0; a < 4; ++a) qx[v][a] = (P)1.0;
         }
-        st4s(&sm.u[v][sw(4 * l, swz)], w);
+        st4s(&sm.u[v][sw(4 * l, swz)], qx[v]);
     }
     __syncthreads();
 
@@ -673,9 +731,9 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     P tr[3][2][NV];   // own face values of this thread's lines (kept only for f32 state arithmetic)
     C jx[2][NV];      // this x-line's x-face corrections
     C fi[3][NV];      // interface fluxes at the minus faces of this thread's lines
-    line_pass<M, FLUX, 0>(A, sm, l, li, nxm, nxp, tr[0][0], tr[0][1], jx, fi[0]);
-    line_pass<M, FLUX, 1>(A, sm, l, li, nym, nyp, tr[1][0], tr[1][1], jx, fi[1]);
-    line_pass<M, FLUX, 2>(A, sm, l, li, nzm, nzp, tr[2][0], tr[2][1], jx, fi[2]);
+    line_pass<M, FLUX, 0>(A, sm, ec, l, li, live, nxm, nxp, tr[0][0], tr[0][1], jx, fi[0], qx);
+    line_pass<M, FLUX, 1>(A, sm, ec, l, li, live, nym, nyp, tr[1][0], tr[1][1], jx, fi[1], qx);
+    line_pass<M, FLUX, 2>(A, sm, ec, l, li, live, nzm, nzp, tr[2][0], tr[2][1], jx, fi[2], qx);
     __syncthreads();
 
     // ---- P5: viscous face fluxes of all six faces, face records
@@ -685,7 +743,15 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     __syncthreads();
 
     // ---- P6: pointwise fluxes of the x-line's points (own points only; the
-    // point order is rotated by k so the 16 lanes of an element hit distinct banks)
+    // point order is rotated by k so the 16 lanes of an element hit distinct
+    // banks). F_y, F_z -> smem for the y / z divergences; the x-line's F_x
+    // never leaves the thread: its x-divergence is accumulated here (point i
+    // contributes column i of the x derivative) and kept until P8.
+    C divx[NV][4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) divx[v][a] = (C)0;
     {
         const int lk = l >> 2;
 #pragma unroll 1
@@ -706,21 +772,25 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
             for (int v = 0; v < NV; ++v) {
                 sm.g[v][p] = F[1][v];
                 sm.g[5 + v][p] = F[2][v];
-                sm.g[10 + v][p] = F[0][v];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const C d = A.sc.d[0][a * 4 + i];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) divx[v][a] = fma(d, F[0][v], divx[v][a]);
             }
         }
     }
     __syncthreads();
 
-    // ---- P7: divergences: x in place (rows 10-14), y -> state region, z in place (rows 5-9)
+    // ---- P7: divergences: y -> state region, z in place (rows 5-9)
     C* divy = reinterpret_cast<C*>(&sm.u[0][0]);
-    div_pass<0, C>(&sm.g[10][0], &sm.g[10][0], li, A.sc.d[0]);
     div_pass<1, C>(&sm.g[0][0], divy, li, A.sc.d[1]);
     div_pass<2, C>(&sm.g[5][0], &sm.g[5][0], li, A.sc.d[2]);
     __syncthreads();
 
     // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
-    if (live) stage_a_update(A, sm, ec, l, swz, divy, jx);
+    if (live) stage_a_update(A, sm, ec, l, swz, divx, divy, jx);
 }
 
 template <class S, class P, class C, class M, int FLUX, int EPB>

@@ -26,7 +26,6 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF_SRC = os.environ.get("OD_REFERENCE_TREE", "/root/reference")
 CUDA_FILES = ("constants.cuh", "device_functions.cuh", "rhs.cu", "rk.cu")  # solver.rs:437-443 order
 HARNESS_SRC = os.path.join(HERE, "ref_harness.cpp")
 HARNESS_SO = os.path.join(OUT, "libodref.so")
@@ -102,10 +101,19 @@ def compile_variant(source: str, v, dest: str) -> None:
     os.replace(tmp, dest)
 
 
-def reference_source() -> str:
+def reference_tree(tree: str | None = None) -> str:
+    """The reference source tree: the argument, else $OD_REFERENCE_TREE."""
+    tree = tree or os.environ.get("OD_REFERENCE_TREE")
+    if not tree:
+        raise FileNotFoundError("no reference tree given (argument or OD_REFERENCE_TREE); "
+                                f"using the prebuilt modules in {OUT}")
+    return tree
+
+
+def reference_source(tree: str) -> str:
     parts = []
     for f in CUDA_FILES:
-        with open(os.path.join(REF_SRC, "src", "cuda", f)) as fh:
+        with open(os.path.join(tree, "src", "cuda", f)) as fh:
             parts.append(fh.read())
     return "\n".join(parts)  # format!("{}\n{}\n{}\n{}", ...)
 
@@ -120,13 +128,14 @@ def build_harness(force: bool = False) -> str:
     return HARNESS_SO
 
 
-def build(force: bool = False) -> None:
+def build(force: bool = False, tree: str | None = None) -> None:
     os.makedirs(OUT, exist_ok=True)
     build_harness(force)
-    if not os.path.isdir(os.path.join(REF_SRC, "src", "cuda")):
-        raise FileNotFoundError(f"reference tree not found at {REF_SRC}; using the prebuilt modules in {OUT}")
-    src = reference_source()
-    src_mtime = max(os.path.getmtime(os.path.join(REF_SRC, "src", "cuda", f)) for f in CUDA_FILES)
+    tree = reference_tree(tree)
+    if not os.path.isdir(os.path.join(tree, "src", "cuda")):
+        raise FileNotFoundError(f"reference tree not found at {tree}; using the prebuilt modules in {OUT}")
+    src = reference_source(tree)
+    src_mtime = max(os.path.getmtime(os.path.join(tree, "src", "cuda", f)) for f in CUDA_FILES)
     for v in variants():
         dest = ptx_path(*v)
         if force or not os.path.exists(dest) or os.path.getmtime(dest) < src_mtime:
@@ -135,4 +144,5 @@ def build(force: bool = False) -> None:
 
 if __name__ == "__main__":
     import sys
-    build(force="--force" in sys.argv)
+    args = [a for a in sys.argv[1:] if a != "--force"]
+    build(force="--force" in sys.argv, tree=args[0] if args else None)

@@ -127,4 +127,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OD_REFERENCE_TREE")
+    if not tree:
+        raise SystemExit("usage: python tests/golden/make_xdmf_golden.py REFERENCE_TREE (or set OD_REFERENCE_TREE)")
+    main(tree)
