@@ -421,9 +421,45 @@ __device__ __forceinline__ void row_line_store(T* row, const LineIdx& li, const 
     }
 }
 
+// Viscous part at one face point: j += 1/2 Fv_own; to the face buffer for
+// the neighbour's phase B: F_I - 1/2 Fv_own at a minus face (fi: the
+// interface flux solved in the line pass), Fv_own (components 1..4) at a
+// plus face.
+// REG: the face's correction j is in registers (jreg), else in shared memory.
+template <class M, int D, bool REG, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
+__device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long long e, int l, int side,
+                                             const P* qp, const C* gt, bool live, C* jreg, const C* fi) {
+    const int f = 2 * D + side;
+    C praw;
+    FaceState<C> s = make_face_state<M, C, P>(qp, praw);
+    C fv[NV];
+    viscous_flux<D>(s, praw, gt, viscosity<M>(A.mu, A.suth, s), fv);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        if constexpr (REG)
+            jreg[v] += (C)0.5 * fv[v];
+        else
+            sm.j[f - 2][v][l] += (C)0.5 * fv[v];
+    }
+    if (!live) return;
+    if (side == 0) {
+        C* out = A.fi + ((e * 3 + D) * NV) * NF + l;
+        out[0] = fi[0];
+#pragma unroll
+        for (int v = 1; v < NV; ++v) out[v * NF] = fi[v] - (C)0.5 * fv[v];
+    } else {
+        C* out = A.fv + ((e * 3 + D) * 4) * NF + l;
+#pragma unroll
+        for (int v = 1; v < NV; ++v) out[(v - 1) * NF] = fv[v];
+    }
+}
+
 // P2-P4: one direction of the gradient / face-value pass for line l.
 // qx: the thread's own x-line as P1 loaded it (used by the x pass instead of
-// reading it back from shared memory).
+// reading it back from shared memory). The z pass (the last one, run after
+// the x and y gradients are in shared memory) also does the z faces' viscous
+// part (P5 for z): its normal gradient components are traced from registers
+// and the z-face corrections are stored once, complete.
 template <class M, int FLUX, int D, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, long long e, int l, const LineIdx& li,
                                           bool live, const long long nb0, const long long nb1, P* oL, P* oR,
@@ -502,6 +538,7 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, long lon
     }
     // corrected gradient along the line (BR1): jl g_L' + jr g_R' + D q, all
     // scaled by the Jacobian, as one FMA chain per point
+    C gnL[NV], gnR[NV];   // z pass: face values of the normal gradient components
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         const C jl = (C)((P)0.5 * (nL[v] + oL[v]) - oL[v]);
@@ -518,12 +555,34 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, long lon
             gv[a] = gg;
         }
         row_line_store<D>(sm.g[3 * v + D], li, gv);
+        if constexpr (D == 2) trace4_lr(gv, A.tc.eL, A.tc.eR, gnL[v], gnR[v]);
     }
     // inviscid parts at the two faces of this line; F_I stays in registers
     // until the minus face's viscous flux is known (P5)
     C j0[NV], j1[NV];
     minus_face<M, FLUX, D, P, C>(oL, nL, D == 1 && nb0 < 0, j0, fi, A.flux);
     plus_face<M, D, P, C>(oR, D == 1 && nb1 < 0, j1);
+    if constexpr (D == 2) {
+        // z faces (never walls): the 11 gradient components the z flux reads,
+        // the normal ones from registers, the x / y ones from shared memory
+        C gL[15], gR[15];
+#pragma unroll
+        for (int c = 0; c < 15; ++c) {
+            if (!grad_used<2>(c)) {
+                gL[c] = (C)0;
+                gR[c] = (C)0;
+            } else if (c % 3 == 2) {
+                gL[c] = gnL[c / 3];
+                gR[c] = gnR[c / 3];
+            } else {
+                C w[4];
+                row_line_load<2>(sm.g[c], li, w);
+                trace4_lr(w, A.tc.eL, A.tc.eR, gL[c], gR[c]);
+            }
+        }
+        viscous_face<M, 2, true>(A, sm, e, l, 0, oL, gL, live, j0, fi);
+        viscous_face<M, 2, true>(A, sm, e, l, 1, oR, gR, live, j1, fi);
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         if constexpr (D == 0) {
@@ -533,39 +592,6 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, long lon
             sm.j[2 * D - 2][v][l] = j0[v];
             sm.j[2 * D - 1][v][l] = j1[v];
         }
-    }
-}
-
-// Viscous part at one face point: j += 1/2 Fv_own; to the face buffer for
-// the neighbour's phase B: F_I - 1/2 Fv_own at a minus face (fi: the
-// interface flux solved in the line pass), Fv_own (components 1..4) at a
-// plus face.
-// REG: the face's correction j is in registers (jreg), else in shared memory.
-template <class M, int D, bool REG, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
-__device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long long e, int l, int side,
-                                             const P* qp, const C* gt, bool live, C* jreg, const C* fi) {
-    const int f = 2 * D + side;
-    C praw;
-    FaceState<C> s = make_face_state<M, C, P>(qp, praw);
-    C fv[NV];
-    viscous_flux<D>(s, praw, gt, viscosity<M>(A.mu, A.suth, s), fv);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        if constexpr (REG)
-            jreg[v] += (C)0.5 * fv[v];
-        else
-            sm.j[f - 2][v][l] += (C)0.5 * fv[v];
-    }
-    if (!live) return;
-    if (side == 0) {
-        C* out = A.fi + ((e * 3 + D) * NV) * NF + l;
-        out[0] = fi[0];
-#pragma unroll
-        for (int v = 1; v < NV; ++v) out[v * NF] = fi[v] - (C)0.5 * fv[v];
-    } else {
-        C* out = A.fv + ((e * 3 + D) * 4) * NF + l;
-#pragma unroll
-        for (int v = 1; v < NV; ++v) out[(v - 1) * NF] = fv[v];
     }
 }
 
@@ -733,13 +759,14 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     C fi[3][NV];      // interface fluxes at the minus faces of this thread's lines
     line_pass<M, FLUX, 0>(A, sm, ec, l, li, live, nxm, nxp, tr[0][0], tr[0][1], jx, fi[0], qx);
     line_pass<M, FLUX, 1>(A, sm, ec, l, li, live, nym, nyp, tr[1][0], tr[1][1], jx, fi[1], qx);
+    __syncthreads();   // the x and y gradients, read by the z faces
     line_pass<M, FLUX, 2>(A, sm, ec, l, li, live, nzm, nzp, tr[2][0], tr[2][1], jx, fi[2], qx);
     __syncthreads();
 
-    // ---- P5: viscous face fluxes of all six faces, face records
+    // ---- P5: viscous face fluxes of the x and y faces, face records (the z
+    // faces are done in the z pass)
     face_grad_pass<M, 0>(A, sm, ec, l, li, false, false, live, tr[0][0], tr[0][1], jx, fi[0]);
     face_grad_pass<M, 1>(A, sm, ec, l, li, nym < 0, nyp < 0, live, tr[1][0], tr[1][1], jx, fi[1]);
-    face_grad_pass<M, 2>(A, sm, ec, l, li, false, false, live, tr[2][0], tr[2][1], jx, fi[2]);
     __syncthreads();
 
     // ---- P6: pointwise fluxes of the x-line's points (own points only; the
@@ -793,8 +820,14 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     if (live) stage_a_update(A, sm, ec, l, swz, divx, divy, jx);
 }
 
+// All-f32 kernels: at most 128 registers per thread, so that 8 blocks of 4
+// elements (16 of 2) fit per SM, the occupancy the shared memory allows. f64
+// slots are twice as large, shared memory bounds those kernels first.
+template <class S, class P, class C, int EPB>
+constexpr int stage_a_min_blocks() { return sizeof(S) == 4 && sizeof(P) == 4 && sizeof(C) == 4 ? 32 / EPB : 1; }
+
 template <class S, class P, class C, class M, int FLUX, int EPB>
-__global__ void __launch_bounds__(LPE * EPB) stage_a_kernel(const StageAParams<S, P, C> A) {
+__global__ void __launch_bounds__(LPE * EPB, (stage_a_min_blocks<S, P, C, EPB>())) stage_a_kernel(const StageAParams<S, P, C> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     stage_a_tile<M, FLUX, EPB>(A, smem_raw, blockIdx.x);
 }
