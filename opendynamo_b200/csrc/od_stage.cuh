@@ -342,16 +342,16 @@ __device__ __forceinline__ void wall_face(const FaceState<C>& so, const C* fe, C
     j[2] = pw - fe[2];
 }
 
+// so: the own face state (make_face_state of the own face values).
 template <class M, int FLUX, int D, class P, class C>
-__device__ __forceinline__ void minus_face(const P* own, const P* nbr, bool wall, C* j, C* fi, int rflux) {
-    C praw;
-    FaceState<C> so = make_face_state<M, C, P>(own, praw);
+__device__ __forceinline__ void minus_face(const FaceState<C>& so, const P* nbr, bool wall, C* j, C* fi, int rflux) {
     C fe[NV];
     euler_flux<D>(so, fe);
     if (wall) {
         wall_face<M, D, P, C>(so, fe, j);
         return;
     }
+    C praw;
     FaceState<C> sn = make_face_state<M, C, P>(nbr, praw);
     if constexpr (FLUX == kFluxRuntime)
         interface_flux_rt<M, D>(rflux, sn, so, fi);
@@ -362,9 +362,7 @@ __device__ __forceinline__ void minus_face(const P* own, const P* nbr, bool wall
 }
 
 template <class M, int D, class P, class C>
-__device__ __forceinline__ void plus_face(const P* own, bool wall, C* j) {
-    C praw;
-    FaceState<C> so = make_face_state<M, C, P>(own, praw);
+__device__ __forceinline__ void plus_face(const FaceState<C>& so, bool wall, C* j) {
     C fe[NV];
     euler_flux<D>(so, fe);
     if (wall) {
@@ -426,12 +424,12 @@ __device__ __forceinline__ void row_line_store(T* row, const LineIdx& li, const 
 // interface flux solved in the line pass), Fv_own (components 1..4) at a
 // plus face.
 // REG: the face's correction j is in registers (jreg), else in shared memory.
+// s, praw: the face state (make_face_state of the face values).
 template <class M, int D, bool REG, class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long long e, int l, int side,
-                                             const P* qp, const C* gt, bool live, C* jreg, const C* fi) {
+                                             const FaceState<C>& s, C praw, const C* gt, bool live, C* jreg,
+                                             const C* fi) {
     const int f = 2 * D + side;
-    C praw;
-    FaceState<C> s = make_face_state<M, C, P>(qp, praw);
     C fv[NV];
     viscous_flux<D>(s, praw, gt, viscosity<M>(A.mu, A.suth, s), fv);
 #pragma unroll
@@ -560,8 +558,11 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, long lon
     // inviscid parts at the two faces of this line; F_I stays in registers
     // until the minus face's viscous flux is known (P5)
     C j0[NV], j1[NV];
-    minus_face<M, FLUX, D, P, C>(oL, nL, D == 1 && nb0 < 0, j0, fi, A.flux);
-    plus_face<M, D, P, C>(oR, D == 1 && nb1 < 0, j1);
+    C prawL, prawR;
+    const FaceState<C> sL = make_face_state<M, C, P>(oL, prawL);
+    const FaceState<C> sR = make_face_state<M, C, P>(oR, prawR);
+    minus_face<M, FLUX, D, P, C>(sL, nL, D == 1 && nb0 < 0, j0, fi, A.flux);
+    plus_face<M, D, P, C>(sR, D == 1 && nb1 < 0, j1);
     if constexpr (D == 2) {
         // z faces (never walls): the 11 gradient components the z flux reads,
         // the normal ones from registers, the x / y ones from shared memory
@@ -580,8 +581,8 @@ __device__ __forceinline__ void line_pass(const PA& A, SlotA<P, C>& sm, long lon
                 trace4_lr(w, A.tc.eL, A.tc.eR, gL[c], gR[c]);
             }
         }
-        viscous_face<M, 2, true>(A, sm, e, l, 0, oL, gL, live, j0, fi);
-        viscous_face<M, 2, true>(A, sm, e, l, 1, oR, gR, live, j1, fi);
+        viscous_face<M, 2, true>(A, sm, e, l, 0, sL, prawL, gL, live, j0, fi);
+        viscous_face<M, 2, true>(A, sm, e, l, 1, sR, prawR, gR, live, j1, fi);
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -643,15 +644,23 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
             trace4_lr(w, A.tp.eL, A.tp.eR, qL[v], qR[v]);
         }
     }
-    if (!wall0) viscous_face<M, D, D == 0>(A, sm, e, l, 0, qL, gL, live, jx[0], fi);
-    if (!wall1) viscous_face<M, D, D == 0>(A, sm, e, l, 1, qR, gR, live, jx[1], fi);
+    if (!wall0) {
+        C praw;
+        const FaceState<C> st = make_face_state<M, C, P>(qL, praw);
+        viscous_face<M, D, D == 0>(A, sm, e, l, 0, st, praw, gL, live, jx[0], fi);
+    }
+    if (!wall1) {
+        C praw;
+        const FaceState<C> st = make_face_state<M, C, P>(qR, praw);
+        viscous_face<M, D, D == 0>(A, sm, e, l, 1, st, praw, gR, live, jx[1], fi);
+    }
 }
 
 // P7: divergence of F_D along the line of thread l (Dm: the Jacobian-scaled
 // derivative of direction D).
 template <int D, class C, class DM>
 __device__ __forceinline__ void div_pass(const C* F, C* out, const LineIdx& li, const DM& Dm) {
-#pragma unroll
+#pragma unroll 1
     for (int v = 0; v < NV; ++v) {
         C w[4];
         row_line_load<D>(F + v * NE, li, w);
