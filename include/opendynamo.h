@@ -200,6 +200,15 @@ size_t od_slab_halo_bytes(const od_ctx* ctx, int kind, int dir);
 int od_slab_pack(od_ctx* ctx, int stage, int kind, int dir, void* d_dst, void* stream);
 int od_slab_unpack(od_ctx* ctx, int stage, int kind, int dir, const void* d_src, void* stream);
 
+/* n SSP-RK3 steps of a whole decomposed mesh whose n slab contexts are all
+ * in this process (slabs[r] holds the layers just below slabs[r+1]'s; z
+ * periodic; one device or several): every exchange is a device copy
+ * straight from a neighbour's boundary layer into the ghost layer it fills,
+ * ordered across the slabs' streams by events, so the host enqueues a whole
+ * step with no wait. Asynchronous (od_sync each slab). Results equal od_step
+ * on the whole mesh bit for bit. No reference counterpart. */
+int od_slabs_step(od_ctx* const* slabs, int n, int n_steps, double dt);
+
 /* Per-kernel timing: when enabled, every stage records CUDA events around its
  * phase-A and phase-B kernels; od_timing sums the recorded intervals since the
  * last reset (synchronizes the stream). */

@@ -34,7 +34,7 @@ EXPORTS = (
     "od_mlp_set_fused",
     "od_attach_closure", "od_project", "od_closure_features", "od_f32_to_bf16",
     "od_point_fields", "od_fields_save", "od_xdmf_text", "od_xdmf_convert",
-    "od_get_state_async", "od_create_slab", "od_slab_stage", "od_slab_halo_bytes", "od_slab_pack", "od_slab_unpack",
+    "od_get_state_async", "od_create_slab", "od_slab_stage", "od_slab_halo_bytes", "od_slab_pack", "od_slab_unpack", "od_slabs_step",
 )
 
 
@@ -173,6 +173,7 @@ def lib() -> ctypes.CDLL:
         "od_slab_halo_bytes": (sz, [vp, ci, ci]),
         "od_slab_pack": (ci, [vp, ci, ci, ci, vp, vp]),
         "od_slab_unpack": (ci, [vp, ci, ci, ci, vp, vp]),
+        "od_slabs_step": (ci, [ctypes.POINTER(vp), ci, ci, cd]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

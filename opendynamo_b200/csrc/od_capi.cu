@@ -154,6 +154,8 @@ struct od_ctx {
     // owned layers 1 .. nz-2 and a ghost layer below and above, which the
     // caller fills between the phases (od_slab_unpack)
     bool slab = false;
+    int slab_z0 = 0, slab_z1 = 0, mesh_nz = 0;   // owned z-layers [z0, z1) of a mesh of mesh_nz layers
+    cudaEvent_t ev_halo[2] = {nullptr, nullptr};   // od_slabs_step: stage input ready / face records ready
     size_t buf_bytes = 0;     // one state buffer (state_bytes: the owned part the caller sees)
     // od_get_state_async: device snapshot of the state and its two events
     void* snap = nullptr;
@@ -482,6 +484,8 @@ void od_destroy(od_ctx* c) {
     if (c->stream_b) cudaStreamSynchronize(c->stream_b);
     for (auto ev : c->events) cudaEventDestroy(ev);
     for (auto ev : c->slab_ev) cudaEventDestroy(ev);
+    for (auto ev : c->ev_halo)
+        if (ev) cudaEventDestroy(ev);
     for (int b = 0; b < 3; ++b)
         if (c->U[b]) cudaFree(c->U[b]);
     if (c->fv) cudaFree(c->fv);
@@ -591,6 +595,9 @@ int od_create_slab(const od_params* g, int z0, int z1, od_ctx** out) {
     od_ctx* c = *out;
     set_jac(c, g);        // element size of the whole mesh
     c->slab = true;
+    c->slab_z0 = z0;
+    c->slab_z1 = z1;
+    c->mesh_nz = g->nz;
     c->state_bytes = (size_t)p.nx * p.ny * (size_t)(z1 - z0) * 64 * 5 * c->elem_size;
     return OD_OK;
 }
@@ -682,6 +689,79 @@ int od_slab_unpack(od_ctx* c, int stage, int kind, int dir, const void* d_src, v
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     cudaError_t e = cudaMemcpy2DAsync(b.p, b.pitch, d_src, b.width, b.width, b.rows, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return cuda_fail(c, e, "slab halo unpack");
+    return OD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One halo message copied straight from slab `from` (its owned boundary
+// layer) into the ghost layer of slab `to` that it fills, on to's stream:
+// dir 0 travels down (from's lowest owned layer -> to's top ghost), dir 1
+// up (from's highest owned layer -> to's bottom ghost). The two contexts may
+// be on different devices (a peer copy).
+cudaError_t slab_copy(od_ctx* to, od_ctx* from, int stage, int kind, int dir) {
+    const HaloBlock s = halo_block(from, stage, kind, dir == 0 ? 1 : from->p.nz - 2, dir == 0);
+    const HaloBlock d = halo_block(to, stage, kind, dir == 0 ? to->p.nz - 1 : 0, dir == 0);
+    return cudaMemcpy2DAsync(d.p, d.pitch, s.p, s.pitch, s.width, s.rows, cudaMemcpyDefault, to->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int od_slabs_step(od_ctx* const* S, int n, int n_steps, double dt) {
+    if (!S || n <= 0 || n_steps < 0) return OD_ERR_ARG;
+    for (int r = 0; r < n; ++r) {
+        od_ctx* c = S[r];
+        if (!c) return OD_ERR_ARG;
+        if (!c->slab) return fail(c, OD_ERR_STATE, "not a slab context (od_create_slab)");
+        if (!c->have_state) return fail(c, OD_ERR_STATE, "no state set");
+        const od_ctx* b = S[(r + 1) % n];
+        const bool next_ok = r + 1 < n ? b->slab_z0 == c->slab_z1 : (b->slab_z0 == 0 && c->slab_z1 == c->mesh_nz);
+        if (!b->slab || b->p.nx != c->p.nx || b->p.ny != c->p.ny || b->mesh_nz != c->mesh_nz ||
+            b->combo != c->combo || !next_ok)
+            return fail(c, OD_ERR_ARG, "slabs must be one mesh's z-slabs, in z order, covering every layer");
+    }
+    for (int r = 0; r < n; ++r) {
+        od_ctx* c = S[r];
+        if (int rc = set_device(c)) return rc;
+        for (auto& ev : c->ev_halo) {
+            if (ev) continue;
+            cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaEventCreate");
+        }
+    }
+    // Per stage: every slab marks its stage input ready; each copies the two
+    // state layers it needs from its neighbours once they are; phase A; the
+    // same with the z-face records; phase B. A slab never runs more than one
+    // phase ahead of its neighbours, so no buffer is overwritten while a
+    // neighbour still copies from it.
+    for (int it = 0; it < n_steps; ++it) {
+        for (int k = 0; k < 3; ++k) {
+            for (int kind = 0; kind < 2; ++kind) {
+                for (int r = 0; r < n; ++r) {
+                    od_ctx* c = S[r];
+                    if (int rc = set_device(c)) return rc;
+                    cudaError_t e = cudaEventRecord(c->ev_halo[kind], c->stream);
+                    if (e != cudaSuccess) return cuda_fail(c, e, "cudaEventRecord");
+                }
+                for (int r = 0; r < n; ++r) {
+                    od_ctx* c = S[r];
+                    od_ctx* above = S[(r + 1) % n];
+                    od_ctx* below = S[(r + n - 1) % n];
+                    if (int rc = set_device(c)) return rc;
+                    cudaError_t e = cudaStreamWaitEvent(c->stream, above->ev_halo[kind], 0);
+                    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, below->ev_halo[kind], 0);
+                    if (e == cudaSuccess) e = slab_copy(c, above, k, kind, 0);
+                    if (e == cudaSuccess) e = slab_copy(c, below, k, kind, 1);
+                    if (e != cudaSuccess) return cuda_fail(c, e, "slab halo copy");
+                    if (int rc = od_slab_stage(c, k, kind, dt)) return rc;
+                }
+            }
+        }
+    }
     return OD_OK;
 }
 

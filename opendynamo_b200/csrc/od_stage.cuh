@@ -910,36 +910,49 @@ __device__ __forceinline__ BCtx<C> b_ctx(const PB& B, long long e, int l) {
     return x;
 }
 
-// Phase B of variable v on the x-line x.l of element x.e.
-template <bool COH, class PB, class C = typename PB::C_t>
-__device__ __forceinline__ void stage_b_var(const PB& B, const BCtx<C>& x, int v) {
+// Phase B of variable v on the x-line x.l of element x.e, in two halves:
+// b_load gathers everything the update reads (the lifted neighbour terms
+// accumulated from the face records, and the RHS / state values), b_store
+// forms the new state and stores it. A thread that handles several variables
+// issues all their loads before its first store.
+template <class P, class C>
+struct BVar {
+    C acc[4];   // lifted neighbour face terms
+    C r[4];     // deferred RK: phase A's RHS
+    P un[4];    // deferred RK: u_in; otherwise the current u_out
+    P u0[4];
+};
+
+template <bool COH, class PB, class C = typename PB::C_t, class P = typename PB::P_t>
+__device__ __forceinline__ BVar<P, C> b_load(const PB& B, const BCtx<C>& x, int v) {
     using S = typename PB::S_t;
-    using P = typename PB::P_t;
     const Mesh& m = B.m;
     const bool defer = (B.flags & kDeferRK) != 0;
     const long long e = x.e, nxm = x.nxm, nxp = x.nxp, nym = x.nym, nyp = x.nyp, nzm = x.nzm, nzp = x.nzp;
     const int l = x.l, lj = x.lj, lk = x.lk;
     const C hx = x.hx, hy = x.hy, hz = x.hz;
-    C acc[4] = {(C)0, (C)0, (C)0, (C)0};
+    BVar<P, C> d;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d.acc[i] = (C)0;
     // plus faces: the plus neighbours' minus-face records F_I - 1/2 Fv
     {
         const C f0 = ldf<COH>(B.fi + ((nxp * 3 + 0) * NV + v) * NF + l);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) acc[i] = fma(-B.jac[0] * B.tc.gR[i], f0, acc[i]);
+        for (int i = 0; i < 4; ++i) d.acc[i] = fma(-B.jac[0] * B.tc.gR[i], f0, d.acc[i]);
     }
     if (nyp >= 0) {
         C w[4];
         ld4s(B.fi + ((nyp * 3 + 1) * NV + v) * NF + 4 * lk, w);
         const C c = -B.jac[1] * B.tc.gR[lj];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+        for (int i = 0; i < 4; ++i) d.acc[i] = fma(c, w[i], d.acc[i]);
     }
     {
         C w[4];
         ld4s(B.fi + ((nzp * 3 + 2) * NV + v) * NF + 4 * lj, w);
         const C c = -B.jac[2] * B.tc.gR[lk];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+        for (int i = 0; i < 4; ++i) d.acc[i] = fma(c, w[i], d.acc[i]);
     }
     if (v > 0) {
         // minus faces: the minus neighbours' viscous fluxes at their plus faces
@@ -947,50 +960,61 @@ __device__ __forceinline__ void stage_b_var(const PB& B, const BCtx<C>& x, int v
         {
             const C a0 = ldf<COH>(B.fv + ((nxm * 3 + 0) * 4 + q) * NF + l);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(hx * B.tc.gL[i], a0, acc[i]);
+            for (int i = 0; i < 4; ++i) d.acc[i] = fma(hx * B.tc.gL[i], a0, d.acc[i]);
         }
         if (nym >= 0) {
             C w[4];
             ld4s(B.fv + ((nym * 3 + 1) * 4 + q) * NF + 4 * lk, w);
             const C c = hy * B.tc.gL[lj];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+            for (int i = 0; i < 4; ++i) d.acc[i] = fma(c, w[i], d.acc[i]);
         }
         {
             C w[4];
             ld4s(B.fv + ((nzm * 3 + 2) * 4 + q) * NF + 4 * lj, w);
             const C c = hz * B.tc.gL[lk];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = fma(c, w[i], acc[i]);
+            for (int i = 0; i < 4; ++i) d.acc[i] = fma(c, w[i], d.acc[i]);
         }
     }
     const long long off = v * m.npts + e * NE + 4 * l;
+    if (defer) {
+        if constexpr (COH)
+            ldc4<S, C>(B.rhs + off, d.r);
+        else
+            ldg4<S, C>(B.rhs + off, d.r);
+        ldg4<S, P>(B.u_in + off, d.un);
+        if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, d.u0);
+    } else {
+        ldc4<S, P>(B.u_out + off, d.un);
+    }
+    return d;
+}
+
+template <class PB, class C = typename PB::C_t, class P = typename PB::P_t>
+__device__ __forceinline__ void b_store(const PB& B, const BCtx<C>& x, int v, const BVar<P, C>& d) {
+    using S = typename PB::S_t;
+    const bool defer = (B.flags & kDeferRK) != 0;
+    const long long off = v * B.m.npts + x.e * NE + 4 * x.l;
     P out[4];
     if (defer) {
-        C r[4];
-        P un[4], u0v[4];
-        if constexpr (COH)
-            ldc4<S, C>(B.rhs + off, r);
-        else
-            ldg4<S, C>(B.rhs + off, r);
-        ldg4<S, P>(B.u_in + off, un);
-        if (B.flags & kHasU0) ldc4<S, P>(B.u0 + off, u0v);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const C rt = r[i] + acc[i];
-            P o = B.rb * un[i] + B.rc * (P)rt;
-            if (B.flags & kHasU0) o = B.ra * u0v[i] + B.rb * un[i] + B.rc * (P)rt;
+            const C rt = d.r[i] + d.acc[i];
+            P o = B.rb * d.un[i] + B.rc * (P)rt;
+            if (B.flags & kHasU0) o = B.ra * d.u0[i] + B.rb * d.un[i] + B.rc * (P)rt;
             out[i] = o;
         }
     } else {
-        P cur[4];
-        ldc4<S, P>(B.u_out + off, cur);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) out[i] = cur[i] + B.rc * (P)acc[i];
+        for (int i = 0; i < 4; ++i) out[i] = d.un[i] + B.rc * (P)d.acc[i];
     }
-    // stored per variable: holding all five (20 more registers) cut the
-    // occupancy and measured 20% slower
     stg4<S, P>(B.u_out + off, out);
+}
+
+template <bool COH, class PB, class C = typename PB::C_t>
+__device__ __forceinline__ void stage_b_var(const PB& B, const BCtx<C>& x, int v) {
+    b_store(B, x, v, b_load<COH>(B, x, v));
 }
 
 // One tile of phase B: EPB elements starting at B.e0 + tile * EPB, 16
@@ -1003,8 +1027,15 @@ __device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
     const long long e = B.e0 + tile * EPB + threadIdx.x / LPE;
     if (e >= B.e1) return;
     const auto x = b_ctx(B, e, l);
+    // all five variables' loads first (memory-level parallelism at phase A's
+    // occupancy inside the persistent ensemble kernel), then the stores
+    using P = typename PB::P_t;
+    using C = typename PB::C_t;
+    BVar<P, C> d[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) stage_b_var<COH>(B, x, v);
+    for (int v = 0; v < NV; ++v) d[v] = b_load<COH>(B, x, v);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) b_store(B, x, v, d[v]);
 }
 
 template <class S, class P, class C, int EPB>

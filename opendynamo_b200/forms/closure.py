@@ -430,7 +430,7 @@ def train(data, cfg, device=0, log=print, net=None):
     return net, {"history": hist, "train_s": time.perf_counter() - t0, "steps": step, "best_val": best[0]}
 
 
-def calibrate(net, data, cfg, device=0, log=print, alphas=(1.0, 0.5, 0.25, 0.125)):
+def calibrate(net, data, cfg, device=0, log=print, alphas=(1.0, 0.75, 0.5, 0.375, 0.25, 0.125)):
     """A posteriori gain of the correction: the coarse run of the last
     training seed (the validation seed) with rhs += alpha * correction for
     each alpha, compared with that seed's filtered fine state at the end of

@@ -10,7 +10,7 @@ stage, so the decomposed run equals it bit for bit.
 Exchanges (the same messages either way):
 
 * ``LocalSlabs`` — every slab in this process, on one GPU or several; the
-  messages are device copies.
+  messages are device copies, a whole step one library call (od_slabs_step).
 * ``DistSlab`` — one slab per rank over torch.distributed: device buffers for
   backends that take them (NCCL, one GPU per rank, NVLink / NVSwitch), or
   staged through host memory otherwise (gloo; also several ranks on one GPU,
@@ -139,10 +139,12 @@ def _step_slabs(slabs, exchange, n_steps: int, dt: float) -> None:
 
 class LocalSlabs:
     """A mesh decomposed into ``n_slabs`` z-slabs held by this process
-    (devices: one CUDA device per slab, default all on params.device)."""
+    (devices: one CUDA device per slab, default all on params.device). A step
+    is one library call (od_slabs_step): every halo is a device copy from the
+    neighbour's boundary layer straight into the ghost layer, ordered across
+    the slabs' streams by events, with no host wait."""
 
     def __init__(self, params: N.OdParams, n_slabs: int, devices: Optional[Sequence[int]] = None):
-        import torch
         self.params = params
         self.ranges = partition(params.nz, n_slabs)
         devices = list(devices) if devices is not None else [int(params.device)] * n_slabs
@@ -154,13 +156,7 @@ class LocalSlabs:
             p.device = d
             self.slabs.append(Slab(p, z0, z1))
         self.npts_layer = params.nx * params.ny * 64
-        # message buffers: [slab][kind][direction]
-        self._buf = [[[torch.empty(s.halo_bytes(k, d), dtype=torch.uint8, device=s.torch_device)
-                       for d in (DOWN, UP)] for k in KINDS] for s in self.slabs]
-        # ordering between the slabs' streams: nothing waits on the host
-        self._streams = [torch.cuda.ExternalStream(s.stream, device=s.torch_device) for s in self.slabs]
-        self._packed = [[torch.cuda.Event() for _ in KINDS] for _ in self.slabs]
-        self._read = [[None for _ in KINDS] for _ in self.slabs]   # neighbours done reading my buffers
+        self._ctxs = (ctypes.c_void_p * n_slabs)(*[s._ctx.value for s in self.slabs])
 
     def close(self) -> None:
         for s in self.slabs:
@@ -174,38 +170,12 @@ class LocalSlabs:
         parts = [s.get_state().reshape(5, -1) for s in self.slabs]
         return np.concatenate(parts, axis=1).reshape(-1)
 
-    def _exchange(self, stage: int, kind: int) -> None:
-        """Stream-ordered: a slab packs once its neighbours have read its
-        previous messages of this kind, unpacks once they have packed."""
-        import torch
-        n = len(self.slabs)
-        for r, (s, b, st) in enumerate(zip(self.slabs, self._buf, self._streams)):
-            for ev in self._read[r][kind] or ():
-                st.wait_event(ev)
-            s.pack(stage, kind, DOWN, b[kind][DOWN])
-            s.pack(stage, kind, UP, b[kind][UP])
-            self._packed[r][kind].record(st)
-        done = []
-        for r, (s, st) in enumerate(zip(self.slabs, self._streams)):
-            a, b = (r + 1) % n, (r - 1) % n
-            st.wait_event(self._packed[a][kind])
-            st.wait_event(self._packed[b][kind])
-            above, below = self._buf[a][kind][DOWN], self._buf[b][kind][UP]
-            if above.device != s.torch_device or below.device != s.torch_device:
-                with torch.cuda.stream(st):
-                    above = above.to(s.torch_device, non_blocking=True)
-                    below = below.to(s.torch_device, non_blocking=True)
-            s.unpack(stage, kind, DOWN, above)
-            s.unpack(stage, kind, UP, below)
-            ev = torch.cuda.Event()
-            ev.record(st)
-            done.append(ev)
-        for r in range(n):
-            # my buffers are read by the slabs above and below
-            self._read[r][kind] = (done[(r + 1) % n], done[(r - 1) % n])
-
     def step(self, n_steps: int, dt: float) -> None:
-        _step_slabs(self.slabs, self._exchange, n_steps, dt)
+        lib = N.lib()
+        rc = lib.od_slabs_step(self._ctxs, len(self.slabs), int(n_steps), float(dt))
+        if rc != 0:
+            bad = next((s for s in self.slabs if lib.od_last_error(s._ctx)), self.slabs[0])
+            N.check(rc, bad._ctx, "od_slabs_step")
 
     def sync(self) -> None:
         for s in self.slabs:

@@ -78,3 +78,11 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(N, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(N.OdError, match="no CPU fallback"):
         N.lib()
+
+
+def test_slabs_step_rejects_bad_arguments_without_gpu():
+    lib = N.lib()
+    assert lib.od_slabs_step(None, 1, 1, 1e-3) == -1
+    arr = (ctypes.c_void_p * 1)(None)
+    assert lib.od_slabs_step(arr, 1, 1, 1e-3) == -1
+    assert lib.od_slabs_step(arr, 0, 1, 1e-3) == -1
