@@ -696,15 +696,46 @@ int od_slab_unpack(od_ctx* c, int stage, int kind, int dir, const void* d_src, v
 
 namespace {
 
-// One halo message copied straight from slab `from` (its owned boundary
-// layer) into the ghost layer of slab `to` that it fills, on to's stream:
-// dir 0 travels down (from's lowest owned layer -> to's top ghost), dir 1
-// up (from's highest owned layer -> to's bottom ghost). The two contexts may
-// be on different devices (a peer copy).
-cudaError_t slab_copy(od_ctx* to, od_ctx* from, int stage, int kind, int dir) {
-    const HaloBlock s = halo_block(from, stage, kind, dir == 0 ? 1 : from->p.nz - 2, dir == 0);
-    const HaloBlock d = halo_block(to, stage, kind, dir == 0 ? to->p.nz - 1 : 0, dir == 0);
-    return cudaMemcpy2DAsync(d.p, d.pitch, s.p, s.pitch, s.width, s.rows, cudaMemcpyDefault, to->stream);
+// Two strided copies (`rows` rows of `width` bytes, pitches in bytes; every
+// address, width and pitch a multiple of 16) in one launch: blockIdx.y picks
+// the copy, the x blocks stride over its 16-byte words.
+struct HaloCopy {
+    const char* src;
+    char* dst;
+    size_t src_pitch, dst_pitch, width, rows;
+};
+
+__global__ void __launch_bounds__(256) halo_copy_kernel(const HaloCopy c0, const HaloCopy c1) {
+    const HaloCopy& c = blockIdx.y == 0 ? c0 : c1;
+    const size_t per_row = c.width / 16, total = per_row * c.rows;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / per_row, w = i - r * per_row;
+        *reinterpret_cast<uint4*>(c.dst + r * c.dst_pitch + 16 * w) =
+            *reinterpret_cast<const uint4*>(c.src + r * c.src_pitch + 16 * w);
+    }
+}
+
+// The two halo messages of one exchange into slab `to`, on to's stream: dir 0
+// travels down (`above`'s lowest owned layer -> to's top ghost), dir 1 up
+// (`below`'s highest owned layer -> to's bottom ghost). Slabs on the same
+// device: one copy kernel; otherwise two peer copies (cudaMemcpy2DAsync).
+cudaError_t slab_exchange(od_ctx* to, od_ctx* above, od_ctx* below, int stage, int kind) {
+    const HaloBlock sa = halo_block(above, stage, kind, 1, true);
+    const HaloBlock da = halo_block(to, stage, kind, to->p.nz - 1, true);
+    const HaloBlock sb = halo_block(below, stage, kind, below->p.nz - 2, false);
+    const HaloBlock db = halo_block(to, stage, kind, 0, false);
+    if (above->p.device != to->p.device || below->p.device != to->p.device) {
+        cudaError_t e = cudaMemcpy2DAsync(da.p, da.pitch, sa.p, sa.pitch, sa.width, sa.rows, cudaMemcpyDefault,
+                                          to->stream);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy2DAsync(db.p, db.pitch, sb.p, sb.pitch, sb.width, sb.rows, cudaMemcpyDefault, to->stream);
+    }
+    const HaloCopy c0{sa.p, da.p, sa.pitch, da.pitch, sa.width, sa.rows};
+    const HaloCopy c1{sb.p, db.p, sb.pitch, db.pitch, sb.width, sb.rows};
+    const size_t words = std::max(sa.width * sa.rows, sb.width * sb.rows) / 16;
+    const unsigned blocks = (unsigned)std::min<size_t>((words + 255) / 256, 148 * 4);
+    halo_copy_kernel<<<dim3(blocks, 2), 256, 0, to->stream>>>(c0, c1);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -754,8 +785,7 @@ int od_slabs_step(od_ctx* const* S, int n, int n_steps, double dt) {
                     if (int rc = set_device(c)) return rc;
                     cudaError_t e = cudaStreamWaitEvent(c->stream, above->ev_halo[kind], 0);
                     if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, below->ev_halo[kind], 0);
-                    if (e == cudaSuccess) e = slab_copy(c, above, k, kind, 0);
-                    if (e == cudaSuccess) e = slab_copy(c, below, k, kind, 1);
+                    if (e == cudaSuccess) e = slab_exchange(c, above, below, k, kind);
                     if (e != cudaSuccess) return cuda_fail(c, e, "slab halo copy");
                     if (int rc = od_slab_stage(c, k, kind, dt)) return rc;
                 }

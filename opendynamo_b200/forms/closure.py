@@ -313,7 +313,7 @@ def features_device(u, n, box, mean, scale, out):
 DEFAULT = dict(fine=96, coarse=24, mid=48, box=(2 * math.pi, 2.0, math.pi), mach=0.2, re_bulk=3000.0,
                amp_frac=0.05, modes=16, train_seeds=tuple(range(16)), eval_seeds=(100, 101, 102, 103),
                dt_fine=1e-4, horizon_steps=2000, snaps_per_seed=125, epochs=8, batch=8192, lr=1e-3,
-               flux="slau2")
+               flux="slau2", val_seeds=2)
 
 
 def _params(n, cfg, device):
@@ -346,7 +346,8 @@ def generate_data(cfg, device=0, log=print):
     prf = torch.empty_like(uc)
     rc = torch.empty_like(uc)
     mean = scale = None
-    calib = {}
+    n_val = max(1, min(int(cfg.get("val_seeds", 1)), len(seeds) - 1)) if len(seeds) > 1 else 1
+    calib = []   # per validation seed: the projected IC and the filtered fine state at the horizon
     row = 0
     t0 = time.perf_counter()
     dt = float(np.float32(cfg["dt_fine"]))
@@ -354,8 +355,9 @@ def generate_data(cfg, device=0, log=print):
         for si, seed in enumerate(seeds):
             u0 = _fine_ic(cfg, seed)
             set_state_device(fine, u0)
-            if si == len(seeds) - 1:
-                calib["u0"] = project(u0, nc, nc, nc, fac)
+            val = si >= len(seeds) - n_val
+            if val:
+                calib.append({"u0": project(u0, nc, nc, nc, fac)})
             del u0
             for k in range(nsnap):
                 fine.step(every, dt)
@@ -378,9 +380,9 @@ def generate_data(cfg, device=0, log=print):
                 d = (prf - rc).view(5, ne, 64).permute(1, 0, 2).reshape(ne, N_OUT)
                 Traw[row:row + ne] = d
                 row += ne
-                if si == len(seeds) - 1 and k == nsnap - 1:
-                    calib["ref"] = uc.clone()
-                    calib["steps"] = every * nsnap
+                if val and k == nsnap - 1:
+                    calib[-1]["ref"] = uc.clone()
+                    calib[-1]["steps"] = every * nsnap
             log(f"seed {seed}: {nsnap} snapshots, {time.perf_counter() - t0:.1f} s")
     finally:
         fine.close()
@@ -391,16 +393,18 @@ def generate_data(cfg, device=0, log=print):
     del Traw, Tn
     torch.cuda.empty_cache()
     return {"X": X, "T": T, "mean": mean, "scale": scale, "out_scale": out_scale.astype(np.float32),
-            "rows_per_seed": nsnap * ne, "seeds": seeds, "gen_s": time.perf_counter() - t0, "calib": calib}
+            "rows_per_seed": nsnap * ne, "seeds": seeds, "gen_s": time.perf_counter() - t0, "calib": calib,
+            "val_seeds": n_val}
 
 
 def train(data, cfg, device=0, log=print, net=None):
-    """Adam on shuffled minibatches; the last training seed is the validation set."""
+    """Adam on shuffled minibatches; the last data["val_seeds"] seeds are the
+    validation set (not trained on)."""
     import torch
     rng = np.random.default_rng(0)
     per = data["rows_per_seed"]
     n = data["X"].shape[0]
-    n_train = n - per if len(data["seeds"]) > 1 else n
+    n_train = n - data.get("val_seeds", 1) * per if len(data["seeds"]) > 1 else n
     own = net is None
     if own:
         net = Network(max_rows=max(cfg["batch"], cfg["coarse"] ** 3), device=device)
@@ -430,32 +434,38 @@ def train(data, cfg, device=0, log=print, net=None):
     return net, {"history": hist, "train_s": time.perf_counter() - t0, "steps": step, "best_val": best[0]}
 
 
-def calibrate(net, data, cfg, device=0, log=print, alphas=(1.0, 0.75, 0.5, 0.375, 0.25, 0.125)):
-    """A posteriori gain of the correction: the coarse run of the last
-    training seed (the validation seed) with rhs += alpha * correction for
-    each alpha, compared with that seed's filtered fine state at the end of
-    the horizon; keeps the alpha with the smallest Reynolds-stress error
-    (alpha = 0, the plain solver, is the fallback)."""
-    cal = data["calib"]
+def calibrate(net, data, cfg, device=0, log=print,
+              alphas=(1.0, 0.75, 0.5, 0.4375, 0.375, 0.3125, 0.25, 0.125)):
+    """A posteriori gain of the correction: the coarse runs of the validation
+    seeds (held out of training) with rhs += alpha * correction for each
+    alpha, compared with those seeds' filtered fine states at the end of the
+    horizon; keeps the alpha with the smallest Reynolds-stress error averaged
+    over the validation seeds (alpha = 0, the plain solver, is the
+    fallback)."""
+    cals = data["calib"] if isinstance(data["calib"], list) else [data["calib"]]
     nc = cfg["coarse"]
     dt = cfg["dt_fine"] * cfg["fine"] / nc
-    steps = int(round(cal["steps"] * cfg["dt_fine"] / dt))
     s = Solver(_params(nc, cfg, device))
     try:
-        set_state_device(s, cal["ref"])
-        ref = _profiles(s)
+        refs = []
+        for cal in cals:
+            set_state_device(s, cal["ref"])
+            refs.append(_profiles(s))
         results = []
         for a in (0.0,) + tuple(alphas):
             if a > 0:
                 net.set_scaling(data["mean"], data["scale"], a * data["out_scale"])
                 net.attach(s)
-            set_state_device(s, cal["u0"])
-            s.step(steps, float(np.float32(dt)))
-            s.sync()
-            err = _errors(_profiles(s), ref)
+            errs = []
+            for cal, ref in zip(cals, refs):
+                set_state_device(s, cal["u0"])
+                s.step(int(round(cal["steps"] * cfg["dt_fine"] / dt)), float(np.float32(dt)))
+                s.sync()
+                errs.append(_errors(_profiles(s), ref))
             if a > 0:
                 Network.detach(s)
-            ok = np.isfinite(err["stress"]) and np.isfinite(err["mean_u"])
+            err = {"mean_u": float(np.mean([e["mean_u"] for e in errs])),
+                   "stress": float(np.mean([e["stress"] for e in errs]))}
             results.append((a, err))
             log(f"calibration alpha {a}: {err}")
         good = [(e["stress"], a) for a, e in results if np.isfinite(e["stress"])]

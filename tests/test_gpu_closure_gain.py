@@ -25,7 +25,7 @@ WEIGHTS = os.path.join(os.path.dirname(CL.__file__), "closure_channel24.npz")
 def test_closure_beats_plain_coarse_on_held_out_seeds():
     cfg = dict(CL.DEFAULT)
     cfg.update(coarse=12, mid=24, fine=48, dt_fine=2e-4, horizon_steps=800, snaps_per_seed=40,
-               train_seeds=tuple(range(6)), eval_seeds=(100, 101), epochs=4)
+               train_seeds=tuple(range(6)), eval_seeds=(100, 101), epochs=4, val_seeds=1)
     data = CL.generate_data(cfg, log=lambda m: None)
     net, tr = CL.train(data, cfg, log=lambda m: None)
     alpha, _ = CL.calibrate(net, data, cfg, log=lambda m: None)
