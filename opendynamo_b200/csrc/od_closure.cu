@@ -168,13 +168,29 @@ __global__ void __launch_bounds__(64) features_kernel(const T* __restrict__ u, F
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b) ch[5 + 3 * a + b] = (d[1 + a][b] - c[1 + a] * ir * d[0][b]) * ir;
-    bf16* row = TILED ? X + (e >> 7) * (128 * kIn) + od::mlp::tile_off((int)(e & 127), p >> 3) / 2 + (p & 7)
-                      : X + e * kIn + p;
-    constexpr int kStride = TILED ? 128 * 64 : 64;   // elements between channels
+    if constexpr (TILED) {
+        // the element's 14 channels x 64 points through shared memory, then
+        // 16-byte chunks of the tile layout (channel c is K block c of the
+        // element's 128-row tile): 112 stores per element instead of 896
+        __shared__ __align__(16) bf16 st[kChan][64];
 #pragma unroll
-    for (int ch_i = 0; ch_i < kChan; ++ch_i)
-        row[ch_i * kStride] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i],
-                                                              -kClip), kClip));
+        for (int ch_i = 0; ch_i < kChan; ++ch_i)
+            st[ch_i][p] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i], -kClip),
+                                                    kClip));
+        __syncthreads();
+        bf16* tile = X + (e >> 7) * (128 * kIn);
+        for (int q = p; q < kChan * 8; q += 64) {
+            const int ch_i = q >> 3, kc = q & 7;
+            *reinterpret_cast<uint4*>(tile + ch_i * (128 * 64) + od::mlp::tile_off((int)(e & 127), kc) / 2) =
+                *reinterpret_cast<const uint4*>(&st[ch_i][8 * kc]);
+        }
+    } else {
+        bf16* row = X + e * kIn + p;
+#pragma unroll
+        for (int ch_i = 0; ch_i < kChan; ++ch_i)
+            row[ch_i * 64] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i], -kClip),
+                                                       kClip));
+    }
 }
 
 FeatParams feat_params(int nx, int ny, int nz, double lx, double ly, double lz, const float* mean,

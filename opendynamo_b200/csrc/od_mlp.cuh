@@ -132,12 +132,28 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear Units",
+// 2016): gelu(z) = z/2 (1 + tanh(k (z + 0.044715 z^3))), k = sqrt(2/pi), with
+// tanh from the single-instruction tanh.approx.f32 (relative error about
+// 2^-11, below the bf16 rounding the activations get next).
+__device__ __forceinline__ float tanh_fast(float x) {
+    float r;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
+constexpr float kGeluK = 0.7978845608028654f;   // sqrt(2 / pi)
+
+__device__ __forceinline__ float gelu(float z) {
+    const float t = tanh_fast(kGeluK * fmaf(0.044715f * z, z * z, z));
+    return 0.5f * z * (1.0f + t);
+}
+
+// d gelu / dz = (1 + t)/2 + z/2 (1 - t^2) k (1 + 3 * 0.044715 z^2)
 __device__ __forceinline__ float gelu_grad(float z) {
-    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-    const float pdf = 0.3989422804014327f * expf(-0.5f * z * z);
-    return cdf + z * pdf;
+    const float z2 = z * z;
+    const float t = tanh_fast(kGeluK * fmaf(0.044715f * z, z2, z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluK * fmaf(0.134145f, z2, 1.0f);
 }
 
 // smem offset of (row r, 16-byte K chunk kc) inside a tile

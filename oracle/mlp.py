@@ -27,17 +27,18 @@ def bf16(x) -> np.ndarray:
     return b.astype(np.uint32).view(np.float32).astype(np.float64).reshape(a.shape)
 
 
-def _erf(x):
-    from scipy.special import erf
-    return erf(x)
+_K = math.sqrt(2.0 / math.pi)
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel 2016), the device's network
+    activation: z/2 (1 + tanh(k (z + 0.044715 z^3))), k = sqrt(2/pi)."""
+    return 0.5 * z * (1.0 + np.tanh(_K * (z + 0.044715 * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(_K * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _K * (1.0 + 3.0 * 0.044715 * z * z)
 
 
 def init_params(rng, scale=1.0, out_scale=0.1) -> dict:
