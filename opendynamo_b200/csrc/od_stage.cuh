@@ -10,14 +10,18 @@
 // owns the d-line through face point l (l = j+4k for x, i+4k for y, i+4j for
 // z, the reference's face-point numbering), so 1-D operators act on four
 // registers:
-//   P1  the element state (x-lines, 128-bit loads) -> smem
-//   P2-4 per direction: own and neighbour face values (BR1 common solution,
-//        slip-wall mirror rhs.cu:111-114), corrected gradient along the line
+//   P1  the element state (x-lines, 128-bit loads) -> smem; each thread
+//        keeps its own x-line for the x pass
+//   P2-4 per direction (x, y, then z after a barrier): own and neighbour
+//        face values (BR1 common solution, slip-wall mirror
+//        rhs.cu:111-114), corrected gradient along the line
 //        (rhs.cu:373-461); at the minus face of the line the interface flux
 //        F_I is solved once for both sides (j = F_I - Fe_own here, F_I kept
 //        in registers); at the plus face j = -Fe_own (slip wall:
-//        j = [0,0,p_w,0,0] - Fe, complete)
-//   P5  x / y / z faces: gradient at the face (11 components), own viscous
+//        j = [0,0,p_w,0,0] - Fe, complete). The y neighbours' traces come
+//        from one 128-bit load per variable and side and a lane
+//        reduce-scatter; the z pass also does P5 for the z faces.
+//   P5  x / y faces: gradient at the face (11 components), own viscous
 //        flux Fv; j += 1/2 Fv_own; to the face buffer for the neighbours:
 //        F_I - 1/2 Fv_own at the minus faces (all the minus neighbour still
 //        needs at its plus face), Fv_own at the plus faces
