@@ -106,6 +106,14 @@ class RefSolver:
         self._ck(self.L.refh_get_state(self.h, out.ctypes.data_as(ctypes.c_void_p), out.nbytes), "refh_get_state")
         return out
 
+    def set_state_ptr(self, ptr: int, nbytes: int):
+        """Upload from host memory at ptr (e.g. a pinned buffer)."""
+        self._ck(self.L.refh_set_state(self.h, ctypes.c_void_p(ptr), nbytes), "refh_set_state")
+
+    def get_state_ptr(self, ptr: int, nbytes: int):
+        """Download into host memory at ptr (e.g. a pinned buffer)."""
+        self._ck(self.L.refh_get_state(self.h, ctypes.c_void_p(ptr), nbytes), "refh_get_state")
+
     def read(self, which):
         if which <= 1:
             out = np.empty(5 * self.npts, dtype=self.udt)
@@ -191,17 +199,21 @@ def bench_line(args, w, rk_per_step, metric, bytes_per_dof_stage, world=1, rank=
             barrier()
             clk = clocks.stop()
             ms = replicas.max_over_ranks(ms, dist, dev)
-            # e2e: state upload + 50 steps + download per bench step
+            # e2e: state upload + 50 steps + download per bench step, from and
+            # into pinned host buffers (as the project's arm)
+            h_in = torch.from_numpy(u).pin_memory()
+            h_out = torch.empty_like(h_in).pin_memory()
+            nbytes = h_in.numel() * h_in.element_size()
             barrier()
             t0 = time.perf_counter()
             for _ in range(args.steps):
-                r.set_state(u)
+                r.set_state_ptr(h_in.data_ptr(), nbytes)
                 r.step(rk_per_step, w["dt"])
-                out = r.get_state()
+                r.get_state_ptr(h_out.data_ptr(), nbytes)
             barrier()
             e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
             launches = r.launches_per_step * rk_per_step * args.steps
-            finite = bool(np.isfinite(out).all())
+            finite = bool(np.isfinite(h_out.numpy()).all())
         stages = args.steps * rk_per_step * 3
         value = replicas.job_throughput(npts * stages, ms / 1e3, world) / 1e9
         e2e = replicas.job_throughput(npts * stages, e2e_s, world) / 1e9
