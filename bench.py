@@ -387,6 +387,25 @@ def run_closure_form(args, world, rank, local):
             "evaluation": ev, "normalisation": norm}
 
 
+def run_closure_scan(args, world, rank, local):
+    """Where the plain coarse run leaves the error band: plain 24^3 and 48^3
+    against the filtered 96^3 run at several horizons, held-out seeds."""
+    if rank != 0:
+        return None
+    import torch
+    from opendynamo_b200.forms import closure as CL
+    torch.cuda.set_device(local)
+    cfg = dict(CL.DEFAULT)
+    marks = [2000, 3000, 4000, 6000, 8000, 12000]
+    rows = CL.plain_error_scan(cfg, marks, device=local, log=lambda m: print(m, file=sys.stderr, flush=True))
+    first_out = next((r["t"] for r in rows if r["plain_coarse"]["stress_mean"] > 0.05), None)
+    return {"metric": "first horizon at which plain 24^3 leaves the 5% Reynolds-stress band (filtered 96^3)",
+            "value": first_out, "unit": "t", "n_gpus": 1, "higher_is_better": False, "dtype": "f32",
+            "data": "synthetic (channel trip ICs, held-out seeds 100-103)",
+            "config": {"workload": "channel 24^3 / 48^3 / 96^3, Re_bulk 3000, Mach 0.2, SLAU2",
+                       "form": "closure-scan"}, "scan": rows}
+
+
 def run_closure_step(args, world, rank, local):
     """Cost of the learned closure inside the step: the coarse channel (24^3 by
     default) stepped with and without the network attached (random weights,
@@ -492,7 +511,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="plain",
-                    choices=["plain", "precision", "ensemble", "closure", "closure-step", "slabs"],
+                    choices=["plain", "precision", "ensemble", "closure", "closure-step", "closure-scan", "slabs"],
                     help="plain: the headline 48^3 bench; precision: the precision-form study")
     ap.add_argument("--physics", default="reference", choices=["reference", "sutherland"],
                     help="plain form: the reference's constant mu = 1.6e-4 (the compared workload) or "
@@ -519,6 +538,8 @@ def main():
         out = run_closure_form(args, world, rank, local)
     elif args.form == "closure-step":
         out = run_closure_step(args, world, rank, local)
+    elif args.form == "closure-scan":
+        out = run_closure_scan(args, world, rank, local)
     elif args.form == "slabs":
         out = run_slabs_form(args, world, rank, local)
     else:

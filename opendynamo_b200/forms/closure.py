@@ -560,6 +560,54 @@ def evaluate(net, cfg, device=0, log=print):
     return out
 
 
+def plain_error_scan(cfg, marks, device=0, log=print):
+    """Errors of the plain coarse and mid runs against the filtered fine run
+    at several horizons (fine-step counts `marks`, increasing), on the
+    evaluation seeds: where the plain coarse run leaves a given error band."""
+    import torch
+    nf, nc, nm = cfg["fine"], cfg["coarse"], cfg["mid"]
+    dts = {"fine": cfg["dt_fine"], "mid": cfg["dt_fine"] * nf / nm, "coarse": cfg["dt_fine"] * nf / nc}
+    out = {int(m): {"plain_coarse": [], "plain_mid": []} for m in marks}
+    fine = Solver(_params(nf, cfg, device))
+    coarse = Solver(_params(nc, cfg, device))
+    mid = Solver(_params(nm, cfg, device))
+    ref_coarse = Solver(_params(nc, cfg, device))
+    try:
+        for seed in cfg["eval_seeds"]:
+            u0 = _fine_ic(cfg, seed)
+            set_state_device(fine, u0)
+            set_state_device(coarse, project(u0, nc, nc, nc, nf // nc))
+            set_state_device(mid, project(u0, nm, nm, nm, nf // nm))
+            done = 0
+            for m in sorted(out):
+                fine.step(m - done, float(np.float32(dts["fine"])))
+                coarse.step((m - done) * nc // nf, float(np.float32(dts["coarse"])))
+                mid.step((m - done) * nm // nf, float(np.float32(dts["mid"])))
+                done = m
+                uf = torch.empty_like(u0)
+                get_state_device(fine, uf)
+                set_state_device(ref_coarse, project(uf, nc, nc, nc, nf // nc))
+                ref = _profiles(ref_coarse)
+                out[m]["plain_coarse"].append(_errors(_profiles(coarse), ref))
+                um = torch.empty(5 * nm ** 3 * 64, device="cuda")
+                get_state_device(mid, um)
+                set_state_device(ref_coarse, project(um, nc, nc, nc, nm // nc))
+                out[m]["plain_mid"].append(_errors(_profiles(ref_coarse), ref))
+                log(f"seed {seed} t={m * cfg['dt_fine']:.2f}: " + ", ".join(f"{k} {v[-1]}" for k, v in out[m].items()))
+    finally:
+        for s in (fine, coarse, mid, ref_coarse):
+            s.close()
+    rows = []
+    for m in sorted(out):
+        r = {"fine_steps": m, "t": m * cfg["dt_fine"]}
+        for k, v in out[m].items():
+            st = [e["stress"] for e in v]
+            r[k] = {"stress_mean": float(np.mean(st)), "stress_max": float(np.max(st)),
+                    "mean_u_mean": float(np.mean([e["mean_u"] for e in v]))}
+        rows.append(r)
+    return rows
+
+
 def _errors(run, ref):
     mu, st = run
     mu_r, st_r = ref
