@@ -204,30 +204,39 @@ class DistExchange:
         s, d = self.slab, self.dist
         below, above = (self.rank - 1) % self.world, (self.rank + 1) % self.world
         send, recv = self._send[kind], self._recv[kind]
+        # packs, sends / receives and unpacks are ordered on the slab's stream
         s.pack(stage, kind, DOWN, send[DOWN])
         s.pack(stage, kind, UP, send[UP])
-        s.sync()
         if self.world == 1:   # the slab is its own neighbour above and below
             s.unpack(stage, kind, DOWN, send[DOWN])
             s.unpack(stage, kind, UP, send[UP])
             return
+        # down goes to the slab below and fills its top ghost; up goes to the slab above
         if self.host:
+            s.sync()
             out = [send[DOWN].cpu(), send[UP].cpu()]
             inc = [torch.empty_like(recv[DOWN], device="cpu"), torch.empty_like(recv[UP], device="cpu")]
-        else:
-            out, inc = send, recv
-        # down goes to the slab below and fills its top ghost; up goes to the slab above
-        ops = [d.P2POp(d.isend, out[DOWN], below, tag=2 * kind),
-               d.P2POp(d.isend, out[UP], above, tag=2 * kind + 1),
-               d.P2POp(d.irecv, inc[DOWN], above, tag=2 * kind),
-               d.P2POp(d.irecv, inc[UP], below, tag=2 * kind + 1)]
-        for q in d.batch_isend_irecv(ops):
-            q.wait()
-        if self.host:
+            ops = [d.P2POp(d.isend, out[DOWN], below, tag=2 * kind),
+                   d.P2POp(d.isend, out[UP], above, tag=2 * kind + 1),
+                   d.P2POp(d.irecv, inc[DOWN], above, tag=2 * kind),
+                   d.P2POp(d.irecv, inc[UP], below, tag=2 * kind + 1)]
+            for q in d.batch_isend_irecv(ops):
+                q.wait()
             recv[DOWN].copy_(inc[DOWN])
             recv[UP].copy_(inc[UP])
-        if recv[DOWN].is_cuda:
-            torch.cuda.synchronize(recv[DOWN].device)
+            if recv[DOWN].is_cuda:
+                torch.cuda.synchronize(recv[DOWN].device)
+        else:
+            # device buffers (NCCL): the collectives run behind the packs on
+            # the slab's stream and the unpacks behind them, no host wait
+            st = torch.cuda.ExternalStream(s.stream, device=s.torch_device)
+            with torch.cuda.stream(st):
+                ops = [d.P2POp(d.isend, send[DOWN], below, tag=2 * kind),
+                       d.P2POp(d.isend, send[UP], above, tag=2 * kind + 1),
+                       d.P2POp(d.irecv, recv[DOWN], above, tag=2 * kind),
+                       d.P2POp(d.irecv, recv[UP], below, tag=2 * kind + 1)]
+                for q in d.batch_isend_irecv(ops):
+                    q.wait()
         s.unpack(stage, kind, DOWN, recv[DOWN])
         s.unpack(stage, kind, UP, recv[UP])
 
