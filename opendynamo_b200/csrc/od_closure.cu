@@ -128,15 +128,10 @@ struct FeatParams {
     float mean[kChan], inv_scale[kChan];
 };
 
-// X: row-major [element][channel * 64 + point], or (TILED) the fused
-// inference kernel's layout: per 128-element tile, per channel (one 64-wide
-// K block) the 128 x 64 block in the shared-memory core-matrix layout, so
-// that one bulk copy fills a feature stage.
-template <class T, bool TILED = false>
+// X: row-major [element][channel * 64 + point]; a thread per point.
+template <class T>
 __global__ void __launch_bounds__(64) features_kernel(const T* __restrict__ u, FeatParams fp, bf16* __restrict__ X) {
     __shared__ float q[4][64];
-    // (tiled: the fused inference kernel that follows may start its prologue now)
-    if (TILED) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const long long e = blockIdx.x;
     const long long npts = (long long)fp.nx * fp.ny * fp.nz * 64;
     const int p = threadIdx.x, i = p & 3, j = (p >> 2) & 3, k = p >> 4;
@@ -168,28 +163,94 @@ __global__ void __launch_bounds__(64) features_kernel(const T* __restrict__ u, F
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b) ch[5 + 3 * a + b] = (d[1 + a][b] - c[1 + a] * ir * d[0][b]) * ir;
-    if constexpr (TILED) {
-        // the element's 14 channels x 64 points through shared memory, then
-        // 16-byte chunks of the tile layout (channel c is K block c of the
-        // element's 128-row tile): 112 stores per element instead of 896
-        __shared__ __align__(16) bf16 st[kChan][64];
+    bf16* row = X + e * kIn + p;
 #pragma unroll
-        for (int ch_i = 0; ch_i < kChan; ++ch_i)
-            st[ch_i][p] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i], -kClip),
-                                                    kClip));
-        __syncthreads();
-        bf16* tile = X + (e >> 7) * (128 * kIn);
-        for (int q = p; q < kChan * 8; q += 64) {
-            const int ch_i = q >> 3, kc = q & 7;
-            *reinterpret_cast<uint4*>(tile + ch_i * (128 * 64) + od::mlp::tile_off((int)(e & 127), kc) / 2) =
-                *reinterpret_cast<const uint4*>(&st[ch_i][8 * kc]);
+    for (int ch_i = 0; ch_i < kChan; ++ch_i)
+        row[ch_i * 64] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i], -kClip),
+                                                   kClip));
+}
+
+// The same features for the fused inference kernel, written in its layout:
+// per 128-element tile, per channel (one 64-wide K block) the 128 x 64 block
+// in the shared-memory core-matrix layout, so that one bulk copy fills a
+// feature stage. f32 state. 16 threads per element, 4 elements per block:
+// thread l owns the x-line (j, k) = (l & 3, l >> 2) of its element, takes the
+// x derivatives of its four points in registers and the y / z derivatives
+// from the four x-lines of its k-plane / j-column in shared memory (128-bit
+// loads), in the same operation order as features_kernel. The channels are
+// staged in shared memory and stored as 16-byte chunks.
+constexpr int kFeatEpb = 4;
+
+__global__ void __launch_bounds__(16 * kFeatEpb) features_tiled_kernel(const float* __restrict__ u, FeatParams fp,
+                                                                        bf16* __restrict__ X, long long nelem) {
+    __shared__ __align__(16) float q[kFeatEpb][4][64];
+    __shared__ __align__(16) bf16 st[kFeatEpb][kChan][64];
+    // the fused inference kernel that follows may start its prologue now
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int es = threadIdx.x >> 4, l = threadIdx.x & 15, j = l & 3, k = l >> 2;
+    const long long e = (long long)blockIdx.x * kFeatEpb + es;
+    const bool live = e < nelem;
+    const long long ec = live ? e : 0;
+    const long long npts = (long long)fp.nx * fp.ny * fp.nz * 64;
+    float c[5][4];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        const float4 w = __ldg(reinterpret_cast<const float4*>(u + v * npts + ec * 64 + 4 * l));
+        c[v][0] = w.x;
+        c[v][1] = w.y;
+        c[v][2] = w.z;
+        c[v][3] = w.w;
+        if (v < 4) *reinterpret_cast<float4*>(&q[es][v][4 * l]) = w;
+    }
+    __syncthreads();
+    float d[4][3][4];   // [var][direction][point of the line]
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        float ly[4][4], lz[4][4];   // the x-lines (m, k) and (j, m), m = 0..3
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const float4 a = *reinterpret_cast<const float4*>(&q[es][v][4 * (m + 4 * k)]);
+            const float4 b = *reinterpret_cast<const float4*>(&q[es][v][4 * (j + 4 * m)]);
+            ly[m][0] = a.x; ly[m][1] = a.y; ly[m][2] = a.z; ly[m][3] = a.w;
+            lz[m][0] = b.x; lz[m][1] = b.y; lz[m][2] = b.z; lz[m][3] = b.w;
         }
-    } else {
-        bf16* row = X + e * kIn + p;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                sx += fp.D[i * 4 + m] * c[v][m];
+                sy += fp.D[j * 4 + m] * ly[m][i];
+                sz += fp.D[k * 4 + m] * lz[m][i];
+            }
+            d[v][0][i] = sx * fp.jac[0];
+            d[v][1][i] = sy * fp.jac[1];
+            d[v][2][i] = sz * fp.jac[2];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int p = i + 4 * l;
+        const float ir = 1.0f / c[0][i];
+        float ch[kChan];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) ch[v] = c[v][i];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) ch[5 + 3 * a + b] = (d[1 + a][b][i] - c[1 + a][i] * ir * d[0][b][i]) * ir;
 #pragma unroll
         for (int ch_i = 0; ch_i < kChan; ++ch_i)
-            row[ch_i * 64] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i], -kClip),
-                                                       kClip));
+            st[es][ch_i][p] = __float2bfloat16_rn(fminf(fmaxf((ch[ch_i] - fp.mean[ch_i]) * fp.inv_scale[ch_i], -kClip),
+                                                        kClip));
+    }
+    __syncthreads();
+    if (!live) return;
+    bf16* tile = X + (e >> 7) * (128 * kIn);
+    for (int q8 = l; q8 < kChan * 8; q8 += 16) {
+        const int ch_i = q8 >> 3, kc = q8 & 7;
+        *reinterpret_cast<uint4*>(tile + ch_i * (128 * 64) + od::mlp::tile_off((int)(e & 127), kc) / 2) =
+            *reinterpret_cast<const uint4*>(&st[es][ch_i][8 * kc]);
     }
 }
 
@@ -717,7 +778,8 @@ cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStre
     if (m->attached_f64)
         features_kernel<double><<<(unsigned)m->nelem_c, 64, 0, s>>>((const double*)u_in, m->fp, m->Xc);
     else if (m->fused)
-        features_kernel<float, true><<<(unsigned)m->nelem_c, 64, 0, s>>>((const float*)u_in, m->fp, m->Xc);
+        features_tiled_kernel<<<(unsigned)((m->nelem_c + kFeatEpb - 1) / kFeatEpb), 16 * kFeatEpb, 0, s>>>(
+            (const float*)u_in, m->fp, m->Xc, (long long)m->nelem_c);
     else
         features_kernel<float><<<(unsigned)m->nelem_c, 64, 0, s>>>((const float*)u_in, m->fp, m->Xc);
     e = cudaGetLastError();
