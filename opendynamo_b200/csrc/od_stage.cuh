@@ -1031,15 +1031,23 @@ __device__ __forceinline__ void stage_b_tile(const PB& B, long long tile) {
     const long long e = B.e0 + tile * EPB + threadIdx.x / LPE;
     if (e >= B.e1) return;
     const auto x = b_ctx(B, e, l);
-    // all five variables' loads first (memory-level parallelism at phase A's
-    // occupancy inside the persistent ensemble kernel), then the stores
-    using P = typename PB::P_t;
-    using C = typename PB::C_t;
-    BVar<P, C> d[NV];
+    if constexpr (COH) {
+        // inside the persistent ensemble kernel (phase A's occupancy): all
+        // five variables' loads first for memory-level parallelism, then the
+        // stores (6.89 -> 6.05 ms per step on the 64-box ensemble)
+        using P = typename PB::P_t;
+        using C = typename PB::C_t;
+        BVar<P, C> d[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) d[v] = b_load<COH>(B, x, v);
+        for (int v = 0; v < NV; ++v) d[v] = b_load<COH>(B, x, v);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) b_store(B, x, v, d[v]);
+        for (int v = 0; v < NV; ++v) b_store(B, x, v, d[v]);
+    } else {
+        // a launch of its own: one variable at a time keeps the registers,
+        // and with them the occupancy, low
+#pragma unroll
+        for (int v = 0; v < NV; ++v) stage_b_var<COH>(B, x, v);
+    }
 }
 
 template <class S, class P, class C, int EPB>
