@@ -302,6 +302,36 @@ int od_state_load(const char* path, void* planes_out, size_t bytes, int expect_u
 const char* od_state_error(void);
 
 /* ------------------------------------------------------------------------
+ * Initial states (host only, no device work): the reference's IC generator
+ * (scripts/make_initial_state.py:122-241) without Python, plus the
+ * Taylor-Green vortex.
+ * ------------------------------------------------------------------------ */
+enum { OD_IC_CHANNEL = 0, OD_IC_UNIFORM = 1, OD_IC_TAYLOR_GREEN = 2 };
+
+typedef struct od_ic_params {
+    int nx, ny, nz;                /* elements per axis */
+    double lx, ly, lz;             /* [mesh] extents as configured (rounded to f32 here, as the script does) */
+    double mach_bulk;              /* [physics] mach_bulk (Taylor-Green: the velocity amplitude v0) */
+    int initial_condition;         /* OD_IC_* ([physics] initial_condition; Taylor-Green is an extension) */
+    double perturbation_amplitude; /* [physics] perturbation_amplitude (0: no trip) */
+    int perturbation_modes;        /* [physics] perturbation_modes */
+    int perturbation_seed;         /* [physics] perturbation_seed */
+} od_ic_params;
+
+/* Five planes (rho, rho*u, rho*v, rho*w, E) of nx*ny*nz*64 values (double if
+ * u_f64, else float) into `planes` (bytes = 5 * nx*ny*nz*64 * size). Channel
+ * and uniform states in the script's float32 arithmetic: without a trip
+ * they equal the script's bit for bit. The trip's sines and cosines are
+ * correctly rounded float32 values where the script takes numpy's (which
+ * differ in about 15% of arguments), and its hash amplifies such a
+ * difference, so a tripped state is a trip of the same construction and
+ * amplitude, not the script's bits. Taylor-Green (double, on [0,lx]x[0,ly]x
+ * [0,lz]): u = v0 sin x cos y cos z, v = -v0 cos x sin y cos z, w = 0,
+ * rho = 1, p = 1/1.4 + v0^2/16 (cos 2x + cos 2y)(cos 2z + 2).
+ * Replaces: initial_condition / apply_trip of scripts/make_initial_state.py. */
+int od_make_initial_state(const od_ic_params* p, void* planes, size_t bytes, int u_f64);
+
+/* ------------------------------------------------------------------------
  * Post-processing: the ParaView conversion of scripts/h5_to_xdmf.py.
  * ------------------------------------------------------------------------ */
 

@@ -23,7 +23,7 @@ EXPORTS = (
     "od_default_params", "od_params_size", "od_abi_version", "od_create", "od_destroy", "od_state_bytes", "od_set_state", "od_get_state",
     "od_set_state_device", "od_get_state_device", "od_step", "od_rhs", "od_sync", "od_stream",
     "od_launches_per_step", "od_set_launch_shape", "od_set_pipeline_slabs", "od_set_timing", "od_timing", "od_last_error", "od_fr_tables",
-    "od_rhs_noalloc", "od_state_save", "od_state_info", "od_state_load", "od_state_error", "od_run",
+    "od_rhs_noalloc", "od_make_initial_state", "od_state_save", "od_state_info", "od_state_load", "od_state_error", "od_run",
     "od_diagnostics",
     "od_ensemble_create", "od_ensemble_destroy", "od_ensemble_state_bytes", "od_ensemble_set_state",
     "od_ensemble_get_state", "od_ensemble_step", "od_ensemble_set_wait", "od_ensemble_set_shape", "od_ensemble_info",
@@ -50,6 +50,19 @@ class OdParams(ctypes.Structure):
         ("device", ctypes.c_int), ("ref_compat", ctypes.c_int),
         ("viscosity_model", ctypes.c_int), ("t_ref", ctypes.c_double), ("s_suth", ctypes.c_double),
     ]
+
+
+class OdIcParams(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("mach_bulk", ctypes.c_double), ("initial_condition", ctypes.c_int),
+        ("perturbation_amplitude", ctypes.c_double), ("perturbation_modes", ctypes.c_int),
+        ("perturbation_seed", ctypes.c_int),
+    ]
+
+
+OD_IC = {"channel": 0, "uniform": 1, "taylor-green": 2}
 
 
 class OdRunOpts(ctypes.Structure):
@@ -121,6 +134,7 @@ def lib() -> ctypes.CDLL:
         "od_last_error": (ctypes.c_char_p, [vp]),
         "od_fr_tables": (ci, [vp]),
         "od_rhs_noalloc": (ci, [P, vp, vp, sz, vp]),
+        "od_make_initial_state": (ci, [ctypes.POINTER(OdIcParams), vp, sz, ci]),
         "od_state_save": (ci, [ctypes.c_char_p, vp, ci, ci, ci, ci, ctypes.c_ulonglong, cd, cd, cd, cd,
                                ctypes.c_char_p]),
         "od_state_info": (ci, [ctypes.c_char_p, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci),

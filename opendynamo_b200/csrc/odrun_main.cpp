@@ -3,6 +3,11 @@
 // argument), validates it against the reference's schema (src/config.rs)
 // and runs od_run.
 //
+// odrun --make-initial-state [config.toml] writes the config's fresh
+// initial state instead, as the reference's IC script does
+// (scripts/make_initial_state.py:311-356): od_make_initial_state, saved as
+// <output_dir>/<prefix>_<u_real>_000000.h5 at label 0, t = 0.
+//
 // The TOML reader covers what config files of this schema use: [table]
 // headers, key = value with integers, floats, booleans and basic / literal
 // strings, and comments. Unknown keys are ignored (serde's default); missing
@@ -12,10 +17,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <map>
 #include <sstream>
 #include <string>
+#include <vector>
 
 #include "opendynamo.h"
 
@@ -172,7 +179,14 @@ std::string enum_of(const std::string& v, std::initializer_list<const char*> all
 }  // namespace
 
 int main(int argc, char** argv) {
-    const char* path = argc > 1 ? argv[1] : "config.toml";
+    bool make_ic = false;
+    const char* path = "config.toml";
+    for (int i = 1; i < argc; ++i) {
+        if (std::strcmp(argv[i], "--make-initial-state") == 0)
+            make_ic = true;
+        else
+            path = argv[i];
+    }
     std::ifstream f(path);
     if (!f) die(std::string("Failed to load ") + path);
     std::stringstream ss;
@@ -196,7 +210,9 @@ int main(int argc, char** argv) {
     std::string ybc = R.get("physics", "y_boundary") ? R.str(*R.get("physics", "y_boundary"), "y_boundary") : "wall";
     p.y_wall = enum_of(ybc, {"wall", "periodic"}, "y_boundary") == "wall";
     if (const Value* v = R.get("physics", "viscosity_model")) enum_of(R.str(*v, "viscosity_model"), {"fixed", "sutherland"}, "viscosity_model");
-    if (const Value* v = R.get("physics", "initial_condition")) enum_of(R.str(*v, "initial_condition"), {"channel", "uniform"}, "initial_condition");
+    std::string ic_kind = "channel";
+    if (const Value* v = R.get("physics", "initial_condition"))
+        ic_kind = enum_of(R.str(*v, "initial_condition"), {"channel", "uniform"}, "initial_condition");
     const Value* ist = R.get("physics", "initial_state");
     const std::string initial_state = ist ? R.str(*ist, "initial_state") : "";
     // [solver]
@@ -246,6 +262,39 @@ int main(int argc, char** argv) {
         const double re = R.number(*v, "re_bulk");
         if (!(re > 0)) die("[b200] re_bulk must be a positive number");
         p.mu = R.f32(R.number(R.req("physics", "mach_bulk"), "mach_bulk")) * (0.5 * p.ly) / re;
+    }
+
+    if (make_ic) {
+        // the script's own defaults for what the config leaves out
+        od_ic_params ic{};
+        ic.nx = p.nx;
+        ic.ny = p.ny;
+        ic.nz = p.nz;
+        ic.lx = p.lx;
+        ic.ly = p.ly;
+        ic.lz = p.lz;
+        ic.mach_bulk = R.number(R.req("physics", "mach_bulk"), "mach_bulk");
+        ic.initial_condition = ic_kind == "uniform" ? OD_IC_UNIFORM : OD_IC_CHANNEL;
+        const Value* amp = R.get("physics", "perturbation_amplitude");
+        const Value* modes = R.get("physics", "perturbation_modes");
+        const Value* seed = R.get("physics", "perturbation_seed");
+        ic.perturbation_amplitude = amp ? R.number(*amp, "perturbation_amplitude") : 0.0;
+        ic.perturbation_modes = modes ? (int)R.integer(*modes, "perturbation_modes") : 16;
+        ic.perturbation_seed = seed ? (int)R.integer(*seed, "perturbation_seed") : 7;
+        const int u_f64 = p.u_real == OD_F64;
+        const size_t n = (size_t)5 * p.nx * p.ny * p.nz * 64;
+        std::vector<double> buf(u_f64 ? n : (n + 1) / 2);
+        if (od_make_initial_state(&ic, buf.data(), n * (u_f64 ? 8 : 4), u_f64) != OD_OK)
+            die("initial state: invalid [mesh] / [physics] values");
+        std::error_code ec;
+        std::filesystem::create_directories(output_dir, ec);
+        if (ec) die("Failed to create output directory " + output_dir + ": " + ec.message());
+        const std::string out = (std::filesystem::path(output_dir) /
+                                 (prefix + (u_f64 ? "_f64" : "_f32") + "_000000.h5")).string();
+        if (od_state_save(out.c_str(), buf.data(), u_f64, p.nx, p.ny, p.nz, 0, 0.0, p.lx, p.ly, p.lz, comp.c_str()) != OD_OK)
+            die(od_state_error());
+        std::printf("Initial state written: %s\n", out.c_str());
+        return 0;
     }
 
     const char* tn[2] = {"F32", "F64"};

@@ -28,7 +28,8 @@ C2RUST = {"int": ("i32", 4), "double": ("f64", 8), "float": ("f32", 4), "long lo
           "unsigned long long": ("u64", 8), "const char*": ("*const c_char", 8), "size_t": ("usize", 8)}
 RUST_SIZE = {r: n for r, n in C2RUST.values()}
 PAIRS = {"OdParams": ("od_params", N.OdParams), "OdRunOpts": ("od_run_opts", N.OdRunOpts),
-         "OdRunResult": ("od_run_result", N.OdRunResult), "OdBox": ("od_box", N.OdBox)}
+         "OdRunResult": ("od_run_result", N.OdRunResult), "OdBox": ("od_box", N.OdBox),
+         "OdIcParams": ("od_ic_params", N.OdIcParams)}
 
 
 def _strip_comments(src: str) -> str:
