@@ -4,7 +4,8 @@
 // One persistent cooperative launch per RK stage covers every box: the grid
 // (sized to what is co-resident: blocks per SM x SM count) strides over the
 // phase-A tiles of all boxes, meets at a grid barrier, then strides over the
-// phase-B tiles. The per-element work is the single-box stage code
+// phase-B tiles. The batched mode runs the same tiles as two ordinary
+// launches per stage (a block per tile), each phase at its own occupancy. The per-element work is the single-box stage code
 // (stage_a_tile / stage_b_tile of od_stage.cuh) with the flux scheme chosen
 // at run time, so every box agrees with advancing it alone with od_step to
 // f32 round-off (the compiler contracts a few multiply-adds differently in
@@ -19,8 +20,9 @@
 // The cooperative launch guarantees co-residency, so the bound is a guard, not
 // a schedule.
 //
-// The autotuner times each candidate shape (elements per block, blocks per
-// SM) on the ensemble itself for a few steps and keeps the fastest.
+// The autotuner times each candidate shape (the batched mode; elements per
+// block and blocks per SM of the persistent launch) on the ensemble itself
+// for a few steps and keeps the fastest.
 
 #include <cuda_runtime.h>
 
@@ -244,6 +246,56 @@ __global__ void __launch_bounds__(LPE * EPB, 16 / EPB * 2) ensemble_stage_kernel
     }
 }
 
+// Batched mode: two ordinary launches per stage over the tiles of every box.
+// Phase A: one tile (EPB elements) per block, at the single-box kernel's
+// occupancy. Phase B: a thread per (element, variable, x-line), two elements
+// per block, as the single-box split kernel. Each launch fills the GPU
+// however small the boxes are, and phase B runs at its own occupancy (the
+// persistent kernel runs it at phase A's); the launches are graph nodes.
+constexpr int kBatchEpbA = 4;
+constexpr int kBatchEpbB = 2;
+
+template <class M, bool CP>
+__global__ void __launch_bounds__(LPE * kBatchEpbA, 32 / kBatchEpbA)
+    ensemble_a_kernel(const EnsBoxStage* __restrict__ boxes, const int2* __restrict__ tile_map) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int2 info = tile_map[blockIdx.x];
+    if constexpr (CP) {
+        od::stage_a_tile<M, od::kFluxRuntime, kBatchEpbA>(c_boxes[info.x].A, smem_raw, info.y);
+    } else {
+        __shared__ __align__(16) StageA As;
+        block_copy(&As, &boxes[info.x].A);
+        __syncthreads();
+        od::stage_a_tile<M, od::kFluxRuntime, kBatchEpbA>(As, smem_raw, info.y);
+    }
+}
+
+template <bool CP>
+__global__ void __launch_bounds__(LPE * od::NV * kBatchEpbB)
+    ensemble_b_kernel(const EnsBoxStage* __restrict__ boxes, const int2* __restrict__ tile_map) {
+    const int2 info = tile_map[blockIdx.x];
+    const int g = threadIdx.x / LPE;
+    const int v = g / kBatchEpbB;
+    const long long e = (long long)info.y * kBatchEpbB + (g - v * kBatchEpbB);
+    const int l = threadIdx.x & (LPE - 1);
+    if constexpr (CP) {
+        const StageB& B = c_boxes[info.x].B;
+        if (e < B.e1) od::stage_b_var<false>(B, od::b_ctx(B, e, l), v);
+    } else {
+        __shared__ __align__(16) StageB Bs;
+        block_copy(&Bs, &boxes[info.x].B);
+        __syncthreads();
+        if (e < Bs.e1) od::stage_b_var<false>(Bs, od::b_ctx(Bs, e, l), v);
+    }
+}
+
+void* batched_a_ptr(bool fast, bool cp) {
+    if (fast) return cp ? (void*)ensemble_a_kernel<od::MathFast, true> : (void*)ensemble_a_kernel<od::MathFast, false>;
+    return cp ? (void*)ensemble_a_kernel<od::MathIeee, true> : (void*)ensemble_a_kernel<od::MathIeee, false>;
+}
+
+void* batched_b_ptr(bool cp) { return cp ? (void*)ensemble_b_kernel<true> : (void*)ensemble_b_kernel<false>; }
+
 template <class M, int EPB>
 void* kernel_ptr(bool cp) {
     return cp ? (void*)ensemble_stage_kernel<M, EPB, true> : (void*)ensemble_stage_kernel<M, EPB, false>;
@@ -275,8 +327,10 @@ struct od_ensemble {
     int2* d_tile_map = nullptr;      // (box, tile in box) of every phase-A tile (sized for 2 elements per tile)
     int2* d_tile_map_b = nullptr;    // the same for the phase-B tiles
     GridSync* d_sync = nullptr;
-    // shape
+    // shape; batched: two ordinary launches per stage instead of the persistent one
     int epb = 4, bps = 0, grid = 0;
+    bool batched = false;
+    long long tiles_a = 0, tiles_b = 0;
     bool use_graph = true, graph_ok = false;
     cudaGraphExec_t exec = nullptr;
     std::string err;
@@ -308,10 +362,13 @@ int build_stage_params(od_ensemble* E) {
     const int nb = (int)E->box.size();
     std::vector<EnsBoxStage> h(nb);
     std::vector<long long> sa(nb + 1, 0), sb(nb + 1, 0);
+    const int eb = E->batched ? kBatchEpbB : E->epb;
     for (int b = 0; b < nb; ++b) {
         sa[b + 1] = sa[b] + (E->nelem[b] + E->epb - 1) / E->epb;
-        sb[b + 1] = sb[b] + (E->nelem[b] + E->epb - 1) / E->epb;
+        sb[b + 1] = sb[b] + (E->nelem[b] + eb - 1) / eb;
     }
+    E->tiles_a = sa[nb];
+    E->tiles_b = sb[nb];
     for (int s = 0; s < 3; ++s) {
         for (int b = 0; b < nb; ++b) {
             const od_box& x = E->box[b];
@@ -387,12 +444,21 @@ int build_stage_params(od_ensemble* E) {
 cudaError_t launch_stage(od_ensemble* E, int s) {
     int nbox = (int)E->box.size();
     const bool cp = nbox <= kConstBoxes;
-    void* fn = pick_kernel(E->fast, E->epb, cp);
     if (cp) {
         cudaError_t c = cudaMemcpyToSymbolAsync(c_boxes, E->d_stage[s], sizeof(EnsBoxStage) * nbox, 0,
                                                 cudaMemcpyDeviceToDevice, E->stream);
         if (c != cudaSuccess) return c;
     }
+    if (E->batched) {
+        void* args_a[] = {(void*)&E->d_stage[s], (void*)&E->d_tile_map};
+        cudaError_t c = cudaLaunchKernel(batched_a_ptr(E->fast, cp), dim3((unsigned)E->tiles_a),
+                                         dim3(LPE * kBatchEpbA), args_a, dyn_smem(kBatchEpbA), E->stream);
+        if (c != cudaSuccess) return c;
+        void* args_b[] = {(void*)&E->d_stage[s], (void*)&E->d_tile_map_b};
+        return cudaLaunchKernel(batched_b_ptr(cp), dim3((unsigned)E->tiles_b), dim3(LPE * od::NV * kBatchEpbB),
+                                args_b, 0, E->stream);
+    }
+    void* fn = pick_kernel(E->fast, E->epb, cp);
     void* args[] = {(void*)&E->d_stage[s], (void*)&nbox, (void*)&E->d_start_a, (void*)&E->d_start_b,
                     (void*)&E->d_tile_map, (void*)&E->d_tile_map_b,
                     (void*)&E->d_sync};
@@ -415,26 +481,32 @@ void drop_graph(od_ensemble* E) {
     E->graph_ok = false;
 }
 
-// set the launch shape; blocks_per_sm <= 0 = as many as are co-resident
+// set the launch shape; blocks_per_sm <= 0 = as many as are co-resident,
+// OD_ENSEMBLE_BATCHED = two ordinary launches per stage (phase A at 4
+// elements per block)
 int apply_shape(od_ensemble* E, int epb, int bps, bool use_graph) {
+    const bool batched = bps == OD_ENSEMBLE_BATCHED;
+    if (batched) epb = kBatchEpbA;
     if (epb != 2 && epb != 4) return efail(E, OD_ERR_ARG, "elements per block must be 2 or 4");
-    void* fn = pick_kernel(E->fast, epb, E->box.size() <= (size_t)kConstBoxes);
+    const bool cp = E->box.size() <= (size_t)kConstBoxes;
+    void* fn = batched ? batched_a_ptr(E->fast, cp) : pick_kernel(E->fast, epb, cp);
     cudaError_t c = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem(epb));
     if (c != cudaSuccess) return ecuda(E, c, "cudaFuncSetAttribute");
     int maxb = 0;
     c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, LPE * epb, dyn_smem(epb));
     if (c != cudaSuccess) return ecuda(E, c, "occupancy");
     if (maxb <= 0) return efail(E, OD_ERR_CUDA, "ensemble kernel cannot be resident");
-    if (bps <= 0 || bps > maxb) bps = maxb;
+    if (!batched && (bps <= 0 || bps > maxb)) bps = maxb;
     drop_graph(E);
-    const bool epb_changed = epb != E->epb;
+    const bool rebuild = epb != E->epb || batched != E->batched || !E->d_stage[0];
     E->epb = epb;
-    E->bps = bps;
-    E->grid = bps * E->nsm;
+    E->batched = batched;
     E->use_graph = use_graph;
-    if (epb_changed || !E->d_stage[0]) {
+    if (rebuild) {
         if (int rc = build_stage_params(E)) return rc;
     }
+    E->bps = batched ? OD_ENSEMBLE_BATCHED : bps;
+    E->grid = batched ? (int)E->tiles_a : bps * E->nsm;
     // a new grid size restarts the arrival counter
     c = cudaMemsetAsync(E->d_sync, 0, sizeof(GridSync), E->stream);
     if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
@@ -544,7 +616,7 @@ int od_ensemble_create(const od_box* boxes, int nbox, int device, int fast_math,
     }
     *out = E;
     E->epb = 0;  // forces the parameter build
-    return apply_shape(E, 4, 0, true);
+    return apply_shape(E, 4, OD_ENSEMBLE_BATCHED, true);   // the faster mode on B200 at every size measured
 }
 
 void od_ensemble_destroy(od_ensemble* E) {
@@ -657,6 +729,7 @@ int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t r
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, LPE * epb, dyn_smem(epb));
         std::vector<int> cands;
         for (int b = maxb; b >= 1; b = b > 2 ? b * 3 / 4 : b - 1) cands.push_back(b);
+        if (epb == kBatchEpbA) cands.insert(cands.begin(), OD_ENSEMBLE_BATCHED);
         for (int bps : cands) {
             if ((rc = apply_shape(E, epb, bps, true))) break;
             if ((rc = enqueue_steps(E, 1))) break;
@@ -667,8 +740,12 @@ int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t r
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
             char line[128];
-            std::snprintf(line, sizeof line, "epb=%d blocks/SM=%d grid=%d graph=%d: %.4f ms/step\n", epb, bps,
-                          E->grid, E->graph_ok ? 1 : 0, ms / trial_steps);
+            if (E->batched)
+                std::snprintf(line, sizeof line, "batched (two launches per stage, %lld + %lld blocks) graph=%d: %.4f ms/step\n",
+                              E->tiles_a, E->tiles_b, E->graph_ok ? 1 : 0, ms / trial_steps);
+            else
+                std::snprintf(line, sizeof line, "epb=%d blocks/SM=%d grid=%d graph=%d: %.4f ms/step\n", epb, bps,
+                              E->grid, E->graph_ok ? 1 : 0, ms / trial_steps);
             rep += line;
             if (ms < best) {
                 best = ms;
@@ -693,7 +770,10 @@ int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t r
     E->steps_done = 0;
     rc = apply_shape(E, best_epb, best_bps, true);
     char line[128];
-    std::snprintf(line, sizeof line, "chosen: epb=%d blocks/SM=%d\n", best_epb, best_bps);
+    if (best_bps == OD_ENSEMBLE_BATCHED)
+        std::snprintf(line, sizeof line, "chosen: batched\n");
+    else
+        std::snprintf(line, sizeof line, "chosen: epb=%d blocks/SM=%d\n", best_epb, best_bps);
     rep += line;
     if (report && report_len) {
         std::strncpy(report, rep.c_str(), report_len - 1);

@@ -78,6 +78,11 @@ def benchmark_boxes(count=64, seed=7, n_min=8, n_max=32, cfl=0.3) -> list[Box]:
     return boxes
 
 
+# blocks_per_sm of set_shape / info for the batched mode: two ordinary
+# launches per stage instead of the persistent one (OD_ENSEMBLE_BATCHED)
+BATCHED = -1
+
+
 class Ensemble:
     """One od_ensemble: boxes advanced together (f32 pipeline)."""
 
@@ -139,6 +144,8 @@ class Ensemble:
                   "od_ensemble_set_wait")
 
     def set_shape(self, elems_per_block: int, blocks_per_sm: int = 0, graph: bool = True):
+        """Persistent launch shape (blocks_per_sm 0: all co-resident), or
+        blocks_per_sm = BATCHED for two launches per stage."""
         self._chk(self._lib.od_ensemble_set_shape(self._h, elems_per_block, blocks_per_sm, int(graph)),
                   "od_ensemble_set_shape")
 

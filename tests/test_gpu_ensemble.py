@@ -1,9 +1,9 @@
 """The batching form on the GPU: boxes of uneven size with mixed schemes,
 walls, viscosities and time steps advanced by one persistent launch per RK
-stage agree box by box with advancing each box alone (to f32 round-off: the
-ensemble kernel contracts a few multiply-adds differently); the grid size and
-the CUDA graph change no bit; the autotuner reports its trials and restores
-the states."""
+stage, or by two batched launches per stage, agree box by box with advancing
+each box alone (to f32 round-off: the ensemble kernels contract a few
+multiply-adds differently); the grid size and the CUDA graph change no bit;
+the autotuner reports its trials and restores the states."""
 
 import math
 
@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from helpers import random_smooth
-from opendynamo_b200.forms.ensemble import Box, Ensemble, benchmark_boxes
+from opendynamo_b200.forms.ensemble import BATCHED, Box, Ensemble, benchmark_boxes
 from opendynamo_b200.solver import Solver
 
 BOXES = [
@@ -89,6 +89,36 @@ def test_ensemble_shape_does_not_change_results(epb):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("graph", [True, False])
+def test_batched_mode_equals_boxes_alone(graph):
+    """Two launches per stage over every box's tiles: the same per-box
+    results, deterministic, and the reported grid is the phase-A tile count."""
+    states = _states(BOXES)
+    want = _alone(BOXES, states, 3)
+    with Ensemble(BOXES) as E:
+        E.set_shape(2, BATCHED, graph)
+        info = E.info()
+        assert info["blocks_per_sm"] == BATCHED and info["elems_per_block"] == 4
+        assert info["grid"] == sum(-(-int(np.prod(b.n)) // 4) for b in BOXES)
+        assert info["graph"] == graph
+        runs = []
+        for _ in range(2):
+            for k, u in enumerate(states):
+                E.set_state(k, u)
+            E.step(3)
+            runs.append([E.get_state(k) for k in range(len(BOXES))])
+        E.set_shape(4, 0, graph)   # back to the persistent launch
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.step(3)
+        persistent = [E.get_state(k) for k in range(len(BOXES))]
+    for k in range(len(BOXES)):
+        _close(runs[0][k], want[k])
+        _close(runs[0][k], persistent[k])
+        assert runs[1][k].tobytes() == runs[0][k].tobytes(), k
+
+
+@pytest.mark.gpu
 def test_autotune_and_benchmark_boxes():
     boxes = benchmark_boxes(count=6, n_min=2, n_max=5)
     assert len({b.flux for b in boxes}) >= 1 and all(2 <= b.n[0] <= 5 for b in boxes)
@@ -98,7 +128,7 @@ def test_autotune_and_benchmark_boxes():
         for k, u in enumerate(states):
             E.set_state(k, u)
         rep = E.autotune(trial_steps=1)
-        assert "chosen:" in rep and "ms/step" in rep
+        assert "chosen:" in rep and "ms/step" in rep and "batched" in rep
         # the autotuner restores the states it stepped
         for k, u in enumerate(states):
             assert E.get_state(k).tobytes() == u.tobytes()
