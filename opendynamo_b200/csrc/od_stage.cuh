@@ -28,7 +28,8 @@
 //   P6  x-threads: pointwise Euler - viscous fluxes of their 4 points
 //        (rhs.cu:229-266); F_y, F_z -> smem, the x-divergence of the
 //        thread's own x-line accumulated in registers
-//   P7  divergence along y and z lines
+//   P7  x-threads: divergence of F_y / F_z at their 4 points from the
+//        x-lines of their k-plane / j-column (128-bit loads)
 //   P8  x-threads: RHS = -div + forcing (rhs.cu:505-509), lifting
 //        -(j_L g_L' + j_R g_R') jac (rk.cu:12-25), RK combination
 //        a*u0 + b*u + c*(RHS + lift) (rk.cu:27-83), 128-bit stores.
@@ -302,8 +303,8 @@ struct SlotBytes {
 // Shared-memory slot of one element in phase A.
 template <class P, class C>
 struct alignas(16) SlotA {
-    C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9; P7: div_z in place
-    P u[NV][NE];          // state; P7: div_y (as C)
+    C g[15][NE];          // gradient; P6: F_y rows 0-4, F_z rows 5-9
+    P u[NV][NE];          // state
     C j[4][NV][NF];       // y / z face corrections without -1/2 Fv_nbr [face - 2][var][face pt]; the x faces of
                           // a line belong to its own thread and stay in registers
     float pad[SlotBytes<P, C>::pad_words];
@@ -660,37 +661,57 @@ __device__ __forceinline__ void face_grad_pass(const PA& A, SlotA<P, C>& sm, lon
     }
 }
 
-// P7: divergence of F_D along the line of thread l (Dm: the Jacobian-scaled
-// derivative of direction D).
-template <int D, class C, class DM>
-__device__ __forceinline__ void div_pass(const C* F, C* out, const LineIdx& li, const DM& Dm) {
-#pragma unroll 1
-    for (int v = 0; v < NV; ++v) {
-        C w[4];
-        row_line_load<D>(F + v * NE, li, w);
-        C r[4];
-        deriv4(w, Dm, r);
-        row_line_store<D>(out + v * NE, li, r);
-    }
-}
-
-// P8 of phase A for one live element: RHS = -div + forcing, own-face lifting
+// P7 + P8 of phase A for one live element: the y / z divergences of the
+// x-line's four points, RHS = -div + forcing, own-face lifting
 // -(j_L g_L' + j_R g_R') jac, then the RK combination, or (deferred RK) the
 // unrounded RHS + own lift for phase B.
+// The y derivative at (i, j, k) reads F_y at (i, 0..3, k): the four x-lines of
+// the thread's k-plane; the z derivative reads F_z at (i, j, 0..3): the four
+// x-lines of its j-column. Each is one 128-bit shared load per x-line (lanes
+// of the same plane / column load the same line: broadcasts), so no pass
+// along y and z lines and no barrier before the update. Operation order per
+// point as a derivative along the line: D[a][0] F_0, then FMAs for m = 1..3.
 template <class PA, class P = typename PA::P_t, class C = typename PA::C_t>
 __device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, long long ec, int l, int swz,
-                                               const C (&divx)[NV][4], const C* divy, const C (&jx)[2][NV]) {
+                                               const C (&divx)[NV][4], const C (&jx)[2][NV]) {
     using S = typename PA::S_t;
     const Mesh& m = A.m;
     const int lj = l & 3, lk = l >> 2;   // this x-line's (j, k)
-    const int px = sw(4 * l, swz);
     const bool defer = (A.flags & kDeferRK) != 0;
+    C cy[4], cz[4];   // derivative rows of this thread's j (y) and k (z)
+#pragma unroll
+    for (int mm = 0; mm < 4; ++mm) {
+        cy[mm] = A.sc.d[1][lj * 4 + mm];
+        cz[mm] = A.sc.d[2][lk * 4 + mm];
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         C dy[4], dz[4], jy0[4], jy1[4], jz0[4], jz1[4];
         const C* dx = divx[v];
-        ld4s(&divy[v * NE + px], dy);
-        ld4s(&sm.g[5 + v][px], dz);
+        {
+            C f[4][4];
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) ld4s(&sm.g[v][sw(4 * (mm + 4 * lk), swz)], f[mm]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                C d = cy[0] * f[0][i];
+#pragma unroll
+                for (int mm = 1; mm < 4; ++mm) d = fma(cy[mm], f[mm][i], d);
+                dy[i] = d;
+            }
+        }
+        {
+            C f[4][4];
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) ld4s(&sm.g[5 + v][sw(4 * (lj + 4 * mm), swz)], f[mm]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                C d = cz[0] * f[0][i];
+#pragma unroll
+                for (int mm = 1; mm < 4; ++mm) d = fma(cz[mm], f[mm][i], d);
+                dz[i] = d;
+            }
+        }
         ld4s(&sm.j[0][v][4 * lk], jy0);
         ld4s(&sm.j[1][v][4 * lk], jy1);
         ld4s(&sm.j[2][v][4 * lj], jz0);
@@ -823,14 +844,9 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     }
     __syncthreads();
 
-    // ---- P7: divergences: y -> state region, z in place (rows 5-9)
-    C* divy = reinterpret_cast<C*>(&sm.u[0][0]);
-    div_pass<1, C>(&sm.g[0][0], divy, li, A.sc.d[1]);
-    div_pass<2, C>(&sm.g[5][0], &sm.g[5][0], li, A.sc.d[2]);
-    __syncthreads();
-
-    // ---- P8: RHS, lifting, RK combination (or the RHS alone for phase B)
-    if (live) stage_a_update(A, sm, ec, l, swz, divx, divy, jx);
+    // ---- P7 + P8: y / z divergences, RHS, lifting, RK combination (or the
+    // RHS alone for phase B)
+    if (live) stage_a_update(A, sm, ec, l, swz, divx, jx);
 }
 
 // All-f32 kernels: at most 128 registers per thread, so that 8 blocks of 4
