@@ -121,6 +121,19 @@ int od_get_state(od_ctx* ctx, void* host, size_t bytes);
  * (src/solver.rs:161-175, 745-759). */
 int od_get_state_async(od_ctx* ctx, void* host, size_t bytes, void* stream);
 
+/* Asynchronous upload: `host` (pinned for a truly asynchronous copy) is
+ * copied to a device staging buffer on `stream`, and the context's stream
+ * takes it over as its state at this point of its order (a device copy); the
+ * call returns at once. The upload may overlap steps enqueued earlier; it
+ * waits, on the device, until the previous asynchronous upload has been taken
+ * over. `host` must stay unchanged until `stream` has passed this point. A
+ * null stream makes it od_set_state. With od_get_state_async on another
+ * stream, a host pipelines independent runs: the next run's upload and the
+ * last run's download overlap the steps in between.
+ * Replaces: the initial-state upload stream.memcpy_htod (src/solver.rs:197-201),
+ * for hosts that run many initial states back to back. */
+int od_set_state_async(od_ctx* ctx, const void* host, size_t bytes, void* stream);
+
 /* Same as above from / to device memory (stream-ordered, no host sync). */
 int od_set_state_device(od_ctx* ctx, const void* dptr, size_t bytes);
 int od_get_state_device(od_ctx* ctx, void* dptr, size_t bytes);

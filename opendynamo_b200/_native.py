@@ -34,7 +34,7 @@ EXPORTS = (
     "od_mlp_set_fused",
     "od_attach_closure", "od_project", "od_closure_features", "od_f32_to_bf16",
     "od_point_fields", "od_fields_save", "od_xdmf_text", "od_xdmf_convert",
-    "od_get_state_async", "od_create_slab", "od_slab_stage", "od_slab_halo_bytes", "od_slab_pack", "od_slab_unpack", "od_slabs_step",
+    "od_get_state_async", "od_set_state_async", "od_create_slab", "od_slab_stage", "od_slab_halo_bytes", "od_slab_pack", "od_slab_unpack", "od_slabs_step",
 )
 
 
@@ -182,6 +182,7 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_ulonglong, cd]),
         "od_xdmf_convert": (ci, [ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_char_p, sz, ctypes.c_char_p, ci]),
         "od_get_state_async": (ci, [vp, vp, sz, vp]),
+        "od_set_state_async": (ci, [vp, vp, sz, vp]),
         "od_create_slab": (ci, [P, ci, ci, ctypes.POINTER(vp)]),
         "od_slab_stage": (ci, [vp, ci, ci, cd]),
         "od_slab_halo_bytes": (sz, [vp, ci, ci]),

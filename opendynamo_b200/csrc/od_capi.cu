@@ -160,6 +160,9 @@ struct od_ctx {
     // od_get_state_async: device snapshot of the state and its two events
     void* snap = nullptr;
     cudaEvent_t ev_snap = nullptr, ev_copied = nullptr;
+    // od_set_state_async: device staging buffer of an upload and its two events
+    void* stage = nullptr;
+    cudaEvent_t ev_staged = nullptr, ev_taken = nullptr;
 };
 
 namespace {
@@ -490,9 +493,15 @@ void od_destroy(od_ctx* c) {
         if (c->U[b]) cudaFree(c->U[b]);
     if (c->fv) cudaFree(c->fv);
     if (c->rhs) cudaFree(c->rhs);
+    // copies still running on the caller's streams
+    if (c->ev_copied) cudaEventSynchronize(c->ev_copied);
+    if (c->ev_staged) cudaEventSynchronize(c->ev_staged);
     if (c->snap) cudaFree(c->snap);
     if (c->ev_snap) cudaEventDestroy(c->ev_snap);
     if (c->ev_copied) cudaEventDestroy(c->ev_copied);
+    if (c->stage) cudaFree(c->stage);
+    if (c->ev_staged) cudaEventDestroy(c->ev_staged);
+    if (c->ev_taken) cudaEventDestroy(c->ev_taken);
     if (c->stream_b) cudaStreamDestroy(c->stream_b);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -547,6 +556,34 @@ int od_get_state_async(od_ctx* c, void* host, size_t bytes, void* stream) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, c->snap, bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaEventRecord(c->ev_copied, s);
     if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous state download");
+    return OD_OK;
+}
+
+int od_set_state_async(od_ctx* c, const void* host, size_t bytes, void* stream) {
+    if (!stream) return od_set_state(c, host, bytes);
+    if (!c || !host) return OD_ERR_ARG;
+    if (bytes != c->state_bytes) return fail(c, OD_ERR_SIZE, "state size does not match the mesh");
+    if (int rc = set_device(c)) return rc;
+    cudaError_t e = cudaSuccess;
+    if (!c->stage) {
+        e = cudaMalloc(&c->stage, c->state_bytes);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_staged, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_taken, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_taken, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "state staging buffer");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    // the caller's stream: once the previous upload has been taken over,
+    // upload into the staging buffer
+    e = cudaStreamWaitEvent(s, c->ev_taken, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->stage, host, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_staged, s);
+    // the compute stream: take the staged state over at this point (a device copy)
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_staged, 0);
+    if (e == cudaSuccess) e = copy_state(c, c->stage, true, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_taken, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous state upload");
+    c->have_state = true;
     return OD_OK;
 }
 

@@ -55,6 +55,9 @@ struct Driver {
     CUresult (*cuMemcpyDtoH)(void*, CUdeviceptr, size_t);
     CUresult (*cuMemcpyHtoDAsync)(CUdeviceptr, const void*, size_t, CUstream);
     CUresult (*cuMemcpyDtoHAsync)(void*, CUdeviceptr, size_t, CUstream);
+    CUresult (*cuMemcpyDtoDAsync)(CUdeviceptr, CUdeviceptr, size_t, CUstream);
+    CUresult (*cuStreamWaitEvent)(CUstream, CUevent, unsigned);
+    CUresult (*cuEventSynchronize)(CUevent);
     CUresult (*cuLaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                                CUstream, void**, void**);
     CUresult (*cuStreamCreate)(CUstream*, unsigned);
@@ -96,6 +99,9 @@ struct Driver {
         SYM(cuMemcpyDtoH, "cuMemcpyDtoH_v2");
         SYM(cuMemcpyHtoDAsync, "cuMemcpyHtoDAsync_v2");
         SYM(cuMemcpyDtoHAsync, "cuMemcpyDtoHAsync_v2");
+        SYM(cuMemcpyDtoDAsync, "cuMemcpyDtoDAsync_v2");
+        SYM(cuStreamWaitEvent, "cuStreamWaitEvent");
+        SYM(cuEventSynchronize, "cuEventSynchronize");
         SYM(cuLaunchKernel, "cuLaunchKernel");
         SYM(cuStreamCreate, "cuStreamCreate");
         SYM(cuStreamDestroy, "cuStreamDestroy_v2");
@@ -196,6 +202,10 @@ struct refh {
     std::string err;
     std::vector<CUevent> ev;
     unsigned rk_block = 1024;  // cudarc for_num_elems; clamped to what the RK kernels can launch
+    // asynchronous host copies (refh_set_state_async / refh_get_state_async):
+    // staging and snapshot buffers with their hand-over events
+    CUdeviceptr stage = 0, snap = 0;
+    CUevent ev_staged = nullptr, ev_taken = nullptr, ev_snap = nullptr, ev_copied = nullptr;
 };
 
 namespace {
@@ -376,7 +386,12 @@ void refh_destroy(refh* h) {
         drv.cuCtxSetCurrent(h->ctx);
         if (h->stream) drv.cuStreamSynchronize(h->stream);
         for (auto e : h->ev) drv.cuEventDestroy(e);
-        CUdeviceptr bufs[] = {h->u, h->u_prev, h->rhs};
+        CUevent aev[] = {h->ev_staged, h->ev_taken, h->ev_snap, h->ev_copied};
+        if (h->ev_staged) drv.cuEventSynchronize(h->ev_staged);
+        if (h->ev_copied) drv.cuEventSynchronize(h->ev_copied);
+        for (auto e : aev)
+            if (e) drv.cuEventDestroy(e);
+        CUdeviceptr bufs[] = {h->u, h->u_prev, h->rhs, h->stage, h->snap};
         for (auto b : bufs)
             if (b) drv.cuMemFree(b);
         for (int q = 0; q < 6; ++q) {
@@ -405,6 +420,52 @@ int refh_get_state(refh* h, void* host, size_t bytes) {
     CK(h, drv.cuCtxSetCurrent(h->ctx), "ctx");
     CK(h, drv.cuMemcpyDtoHAsync(host, h->u, bytes, h->stream), "download");
     CK(h, drv.cuStreamSynchronize(h->stream), "sync");
+    return 0;
+}
+
+// Asynchronous upload on `stream`: host -> staging buffer, then the compute
+// stream takes it over as u at this point of its order (a device copy). The
+// same hand-over as od_set_state_async, so both bench arms pipeline their
+// host copies alike.
+int refh_set_state_async(refh* h, const void* host, size_t bytes, void* stream) {
+    if (!stream) return refh_set_state(h, host, bytes);
+    if (bytes != h->state_size * h->us) return -3;
+    CK(h, drv.cuCtxSetCurrent(h->ctx), "ctx");
+    if (!h->stage) {
+        CK(h, drv.cuMemAlloc(&h->stage, bytes), "alloc staging buffer");
+        CK(h, drv.cuEventCreate(&h->ev_staged, 2 /* CU_EVENT_DISABLE_TIMING */), "event");
+        CK(h, drv.cuEventCreate(&h->ev_taken, 2), "event");
+        CK(h, drv.cuEventRecord(h->ev_taken, h->stream), "event record");
+    }
+    CUstream s = (CUstream)stream;
+    CK(h, drv.cuStreamWaitEvent(s, h->ev_taken, 0), "wait");
+    CK(h, drv.cuMemcpyHtoDAsync(h->stage, host, bytes, s), "upload");
+    CK(h, drv.cuEventRecord(h->ev_staged, s), "event record");
+    CK(h, drv.cuStreamWaitEvent(h->stream, h->ev_staged, 0), "wait");
+    CK(h, drv.cuMemcpyDtoDAsync(h->u, h->stage, bytes, h->stream), "take over");
+    CK(h, drv.cuEventRecord(h->ev_taken, h->stream), "event record");
+    return 0;
+}
+
+// Asynchronous download on `stream` of u as of this point of the compute
+// stream, through a device snapshot (as od_get_state_async).
+int refh_get_state_async(refh* h, void* host, size_t bytes, void* stream) {
+    if (!stream) return refh_get_state(h, host, bytes);
+    if (bytes != h->state_size * h->us) return -3;
+    CK(h, drv.cuCtxSetCurrent(h->ctx), "ctx");
+    if (!h->snap) {
+        CK(h, drv.cuMemAlloc(&h->snap, bytes), "alloc snapshot buffer");
+        CK(h, drv.cuEventCreate(&h->ev_snap, 2), "event");
+        CK(h, drv.cuEventCreate(&h->ev_copied, 2), "event");
+        CK(h, drv.cuEventRecord(h->ev_copied, h->stream), "event record");
+    }
+    CUstream s = (CUstream)stream;
+    CK(h, drv.cuStreamWaitEvent(h->stream, h->ev_copied, 0), "wait");
+    CK(h, drv.cuMemcpyDtoDAsync(h->snap, h->u, bytes, h->stream), "snapshot");
+    CK(h, drv.cuEventRecord(h->ev_snap, h->stream), "event record");
+    CK(h, drv.cuStreamWaitEvent(s, h->ev_snap, 0), "wait");
+    CK(h, drv.cuMemcpyDtoHAsync(host, h->snap, bytes, s), "download");
+    CK(h, drv.cuEventRecord(h->ev_copied, s), "event record");
     return 0;
 }
 

@@ -41,6 +41,8 @@ def lib():
         L.refh_state_bytes.restype = ctypes.c_size_t
         L.refh_set_state.argtypes = [vp, vp, ctypes.c_size_t]
         L.refh_get_state.argtypes = [vp, vp, ctypes.c_size_t]
+        L.refh_set_state_async.argtypes = [vp, vp, ctypes.c_size_t, vp]
+        L.refh_get_state_async.argtypes = [vp, vp, ctypes.c_size_t, vp]
         L.refh_read.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t]
         L.refh_rhs_stage.argtypes = [vp]
         L.refh_rk.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -113,6 +115,17 @@ class RefSolver:
     def get_state_ptr(self, ptr: int, nbytes: int):
         """Download into host memory at ptr (e.g. a pinned buffer)."""
         self._ck(self.L.refh_get_state(self.h, ctypes.c_void_p(ptr), nbytes), "refh_get_state")
+
+    def set_state_async(self, ptr: int, nbytes: int, stream: int):
+        """Upload from pinned host memory on `stream`, taken over in the
+        compute stream's order (refh_set_state_async)."""
+        self._ck(self.L.refh_set_state_async(self.h, ctypes.c_void_p(ptr), nbytes, ctypes.c_void_p(stream)),
+                 "refh_set_state_async")
+
+    def get_state_async(self, ptr: int, nbytes: int, stream: int):
+        """Download of a snapshot of u into pinned host memory on `stream`."""
+        self._ck(self.L.refh_get_state_async(self.h, ctypes.c_void_p(ptr), nbytes, ctypes.c_void_p(stream)),
+                 "refh_get_state_async")
 
     def read(self, which):
         if which <= 1:
@@ -200,10 +213,29 @@ def bench_line(args, w, rk_per_step, metric, bytes_per_dof_stage, world=1, rank=
             clk = clocks.stop()
             ms = replicas.max_over_ranks(ms, dist, dev)
             # e2e: state upload + 50 steps + download per bench step, from and
-            # into pinned host buffers (as the project's arm)
+            # into pinned host buffers, exactly as the project's arm: the
+            # copies pipelined on two copy streams (each bench step's upload
+            # and the previous one's download overlap the steps), and the
+            # same loop with blocking copies
             h_in = torch.from_numpy(u).pin_memory()
             h_out = torch.empty_like(h_in).pin_memory()
             nbytes = h_in.numel() * h_in.element_size()
+            up, down = torch.cuda.Stream(), torch.cuda.Stream()
+
+            def e2e_pipelined(n):
+                for _ in range(n):
+                    r.set_state_async(h_in.data_ptr(), nbytes, up.cuda_stream)
+                    r.step(rk_per_step, w["dt"])
+                    r.get_state_async(h_out.data_ptr(), nbytes, down.cuda_stream)
+                down.synchronize()
+                r.sync()
+
+            e2e_pipelined(1)
+            barrier()
+            t0 = time.perf_counter()
+            e2e_pipelined(args.steps)
+            barrier()
+            e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
             barrier()
             t0 = time.perf_counter()
             for _ in range(args.steps):
@@ -211,12 +243,13 @@ def bench_line(args, w, rk_per_step, metric, bytes_per_dof_stage, world=1, rank=
                 r.step(rk_per_step, w["dt"])
                 r.get_state_ptr(h_out.data_ptr(), nbytes)
             barrier()
-            e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
+            e2e_blocking_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
             launches = r.launches_per_step * rk_per_step * args.steps
             finite = bool(np.isfinite(h_out.numpy()).all())
         stages = args.steps * rk_per_step * 3
         value = replicas.job_throughput(npts * stages, ms / 1e3, world) / 1e9
         e2e = replicas.job_throughput(npts * stages, e2e_s, world) / 1e9
+        e2e_blocking = replicas.job_throughput(npts * stages, e2e_blocking_s, world) / 1e9
         line = {
             "impl": "reference", "metric": metric, "value": round(value, 3), "unit": "Gdof*stage/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -228,7 +261,8 @@ def bench_line(args, w, rk_per_step, metric, bytes_per_dof_stage, world=1, rank=
                               "NVRTC compute_100 --use_fast_math, driver JIT, src/solver.rs launch shapes and "
                               "sequence; it has no CPU path",
             "e2e": {"value": round(e2e, 3), "unit": "Gdof*stage/s", "h2d_bytes_per_step": int(u.nbytes),
-                    "d2h_bytes_per_step": int(u.nbytes)},
+                    "d2h_bytes_per_step": int(u.nbytes), "copies": bench.E2E_COPIES,
+                    "blocking_value": round(e2e_blocking, 3)},
             "gpu_launches": launches, "clocks": clk, "state_finite": finite,
         }
         replicas.finish(dist)

@@ -1,7 +1,10 @@
 """od_get_state_async: the download reads a snapshot taken at its point of
 the context's stream, so steps enqueued right after it do not change what
 arrives; two downloads in a row each get their own state; a slab context
-downloads its owned layers."""
+downloads its owned layers. od_set_state_async: uploads staged on another
+stream are taken over in the context's stream order, so a pipeline of
+independent runs (next upload and last download overlapping the steps)
+gives each run's own result."""
 
 from __future__ import annotations
 
@@ -73,3 +76,33 @@ def test_async_download_of_a_slab():
         assert np.array_equal(h.numpy(), SL.owned_planes(u, 3 * 4 * 64, 2, 5).reshape(-1))
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+def test_async_upload_pipeline_of_independent_runs():
+    import torch
+    mesh = (5, 4, 6)
+    p = make_params(*mesh, 2 * math.pi, 2.0, math.pi, "slau2", True, "f32")
+    dt = float(np.float32(2e-4))
+    states = [channel_trip(*mesh, seed=s, dtype=np.float32) for s in (1, 2, 3)]
+    want = [reference(p, u, 4, dt) for u in states]
+    L = N.lib()
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    with Solver(p) as s:
+        h_in = [torch.from_numpy(u).pin_memory() for u in states]
+        h_out = [torch.empty_like(h).pin_memory() for h in h_in]
+        for k in range(3):
+            assert L.od_set_state_async(s._ctx, ctypes.c_void_p(h_in[k].data_ptr()), s.state_bytes,
+                                        ctypes.c_void_p(up.cuda_stream)) == 0
+            s.step(4, dt)
+            assert L.od_get_state_async(s._ctx, ctypes.c_void_p(h_out[k].data_ptr()), s.state_bytes,
+                                        ctypes.c_void_p(down.cuda_stream)) == 0
+        down.synchronize()
+        s.sync()
+        for k in range(3):
+            assert np.array_equal(h_out[k].numpy(), want[k]), k
+        # a null stream is the blocking upload; a wrong size is refused
+        assert L.od_set_state_async(s._ctx, states[0].ctypes.data_as(ctypes.c_void_p), s.state_bytes, None) == 0
+        assert np.array_equal(s.get_state(), states[0])
+        assert L.od_set_state_async(s._ctx, ctypes.c_void_p(h_in[0].data_ptr()), s.state_bytes - 4,
+                                    ctypes.c_void_p(up.cuda_stream)) == -3
