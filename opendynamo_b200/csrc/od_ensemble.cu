@@ -273,7 +273,8 @@ __global__ void __launch_bounds__(LPE * kBatchEpbA, 32 / kBatchEpbA)
 template <bool CP>
 __global__ void __launch_bounds__(LPE * od::NV * kBatchEpbB)
     ensemble_b_kernel(const EnsBoxStage* __restrict__ boxes, const int2* __restrict__ tile_map) {
-    const int2 info = tile_map[blockIdx.x];
+    // reverse tile order: phase A's last writes are still in L2 (as the single-box phase B)
+    const int2 info = tile_map[gridDim.x - 1 - blockIdx.x];
     const int g = threadIdx.x / LPE;
     const int v = g / kBatchEpbB;
     const long long e = (long long)info.y * kBatchEpbB + (g - v * kBatchEpbB);

@@ -1072,12 +1072,16 @@ __global__ void __launch_bounds__(LPE * EPB) stage_b_kernel(const StageBParams<S
 }
 
 // Phase B with one thread per (element, variable, x-line): 80 threads per
-// element; a warp holds two elements' lines of one variable.
+// element; a warp holds two elements' lines of one variable. Blocks walk
+// the elements in reverse order: phase A's last RHS and face records (the
+// highest elements) are still in L2 when phase B starts, and phase B's last
+// stores (the lowest elements) are what the next phase A reads first
+// (48^3 f32: phase B 120.9 -> 117.5 us, phase A 263.0 -> 262.4 us).
 template <class S, class P, class C, int EPB>
 __global__ void __launch_bounds__(LPE * NV * EPB) stage_b_split_kernel(const StageBParams<S, P, C> B) {
     const int g = threadIdx.x / LPE;
     const int v = g / EPB;
-    const long long e = B.e0 + (long long)blockIdx.x * EPB + (g - v * EPB);
+    const long long e = B.e0 + (long long)(gridDim.x - 1 - blockIdx.x) * EPB + (g - v * EPB);
     if (e >= B.e1) return;
     stage_b_var<false>(B, b_ctx(B, e, threadIdx.x & (LPE - 1)), v);
 }
