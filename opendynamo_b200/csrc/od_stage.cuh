@@ -850,10 +850,17 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
 }
 
 // All-f32 kernels: at most 128 registers per thread, so that 8 blocks of 4
-// elements (16 of 2) fit per SM, the occupancy the shared memory allows. f64
-// slots are twice as large, shared memory bounds those kernels first.
+// elements (16 of 2) fit per SM, the occupancy the shared memory allows.
+// Mixed precision (f64 state, f32 fluxes): 6 blocks of 4 elements, at most
+// 168 registers (left free, the compiler takes 190 and 5 blocks fit: 10%
+// slower at 96^3). Slots with f64 gradients are larger; shared memory bounds
+// those kernels first.
 template <class S, class P, class C, int EPB>
-constexpr int stage_a_min_blocks() { return sizeof(S) == 4 && sizeof(P) == 4 && sizeof(C) == 4 ? 32 / EPB : 1; }
+constexpr int stage_a_min_blocks() {
+    if (sizeof(S) == 4 && sizeof(P) == 4 && sizeof(C) == 4) return 32 / EPB;
+    if (sizeof(S) == 8 && sizeof(P) == 8 && sizeof(C) == 4) return 24 / EPB;
+    return 1;
+}
 
 template <class S, class P, class C, class M, int FLUX, int EPB>
 __global__ void __launch_bounds__(LPE * EPB, (stage_a_min_blocks<S, P, C, EPB>())) stage_a_kernel(const StageAParams<S, P, C> A) {
