@@ -849,15 +849,20 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
     if (live) stage_a_update(A, sm, ec, l, swz, divx, jx);
 }
 
-// All-f32 kernels: at most 128 registers per thread, so that 8 blocks of 4
-// elements (16 of 2) fit per SM, the occupancy the shared memory allows.
-// Mixed precision (f64 state, f32 fluxes): 6 blocks of 4 elements, at most
-// 168 registers (left free, the compiler takes 190 and 5 blocks fit: 10%
-// slower at 96^3). Slots with f64 gradients are larger; shared memory bounds
+// Blocks per SM the register budget is set for. f32 state arithmetic and
+// fluxes (the all-f32 pipeline, and the reference's default of an f64 state
+// with f32 arithmetic): at most 128 registers per thread, so that 8 blocks of
+// 4 elements (16 of 2) fit per SM, the occupancy the shared memory allows
+// (u64/c32 at 64^3: phase A 1161 us at the 5 blocks its free choice of 198
+// registers allowed, 931 us at 8; its SLAU2 fast-math kernel does not spill,
+// some IEEE, AUSM+ and Sutherland variants spill 8-72 bytes). Mixed precision (f64 state, f32
+// fluxes): 6 blocks of 4 elements, at most 168 registers (left free, the
+// compiler takes 190 and 5 blocks fit: 10% slower at 96^3; 7 blocks spill and
+// are 9% slower). Slots with f64 gradients are larger; shared memory bounds
 // those kernels first.
 template <class S, class P, class C, int EPB>
 constexpr int stage_a_min_blocks() {
-    if (sizeof(S) == 4 && sizeof(P) == 4 && sizeof(C) == 4) return 32 / EPB;
+    if (sizeof(P) == 4 && sizeof(C) == 4) return 32 / EPB;
     if (sizeof(S) == 8 && sizeof(P) == 8 && sizeof(C) == 4) return 24 / EPB;
     return 1;
 }
