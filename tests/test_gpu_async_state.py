@@ -61,7 +61,7 @@ def test_async_download_reads_a_snapshot():
 
 
 @pytest.mark.gpu
-def test_async_download_of_a_slab():
+def test_async_transfers_of_a_slab():
     import torch
     p = make_params(3, 4, 6, 2 * math.pi, 2.0, math.pi, "rusanov", False, "f32")
     u = channel_trip(3, 4, 6, dtype=np.float32)
@@ -74,6 +74,14 @@ def test_async_download_of_a_slab():
                                           ctypes.c_void_p(side.cuda_stream)) == 0
         side.synchronize()
         assert np.array_equal(h.numpy(), SL.owned_planes(u, 3 * 4 * 64, 2, 5).reshape(-1))
+        # an asynchronous upload fills the owned layers the same way
+        v = channel_trip(3, 4, 6, seed=9, dtype=np.float32)
+        h_in = torch.from_numpy(np.ascontiguousarray(SL.owned_planes(v, 3 * 4 * 64, 2, 5).reshape(-1))).pin_memory()
+        assert N.lib().od_set_state_async(s._ctx, ctypes.c_void_p(h_in.data_ptr()), s.state_bytes,
+                                          ctypes.c_void_p(side.cuda_stream)) == 0
+        out = np.empty(s.state_bytes // 4, dtype=np.float32)
+        assert N.lib().od_get_state(s._ctx, out.ctypes.data_as(ctypes.c_void_p), out.nbytes) == 0
+        assert np.array_equal(out, h_in.numpy())
     finally:
         s.close()
 
