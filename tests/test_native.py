@@ -63,6 +63,32 @@ def test_create_rejects_bad_arguments():
     p.mixed = 1  # mixed needs u_real = f64
     assert lib.od_create(ctypes.byref(p), ctypes.byref(ctx)) == -1
     assert lib.od_create(None, ctypes.byref(ctx)) == -1
+    # extents, viscosity model, and the 32-bit element index limit
+    for field, value in (("lx", 0.0), ("ly", -1.0), ("lz", float("nan")), ("viscosity_model", 5), ("t_ref", 0.0)):
+        lib.od_default_params(ctypes.byref(p))
+        if field == "t_ref":
+            p.viscosity_model = 1
+        setattr(p, field, value)
+        assert lib.od_create(ctypes.byref(p), ctypes.byref(ctx)) == -1, field
+    lib.od_default_params(ctypes.byref(p))
+    p.nx, p.ny, p.nz = 1300, 1300, 1300   # 2.2e9 elements: above 2^31 - 1
+    assert lib.od_create(ctypes.byref(p), ctypes.byref(ctx)) == -1
+    assert not ctx.value
+
+
+def test_ensemble_create_rejects_bad_boxes_without_gpu():
+    lib = N.lib()
+    good = N.OdBox(2, 2, 2, 1.0, 1.0, 1.0, 0, 1, 1e-3, 0.0, 1e-3)
+    h = ctypes.c_void_p()
+    for field, value in (("nx", 0), ("lx", 0.0), ("flux", 3), ("dt", 0.0), ("mu", -1e-3)):
+        bad = N.OdBox(*[getattr(good, n) for n, _ in N.OdBox._fields_])
+        setattr(bad, field, value)
+        arr = (N.OdBox * 2)(good, bad)
+        assert lib.od_ensemble_create(arr, 2, 0, 1, ctypes.byref(h)) == -1, field
+        assert not h.value
+    arr = (N.OdBox * 1)(good)
+    assert lib.od_ensemble_create(arr, 0, 0, 1, ctypes.byref(h)) == -1
+    assert lib.od_ensemble_create(None, 1, 0, 1, ctypes.byref(h)) == -1
 
 
 def test_null_context_calls_fail_cleanly():
