@@ -92,6 +92,7 @@ struct StageA {
     float jac[3];
     float ra, rb, rc;
     float mu, forcing, suth;
+    float kappa;   // heat-flux coefficient of mu (od::heat_coeff_host)
     int flags;
     int flux;
     long long e0, e1;
@@ -402,6 +403,7 @@ int build_stage_params(od_ensemble* E) {
             A.rb = rb[s];
             A.rc = rc[s];
             A.mu = (float)x.mu;
+            A.kappa = od::heat_coeff_host<float>(A.mu);
             A.forcing = (float)x.forcing;
             A.suth = -1.0f;
             A.flags = od::kDeferRK | (s == 0 ? 0 : od::kHasU0);

@@ -96,6 +96,7 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.rb = (P)L.rb;
     A.rc = (P)L.rc;
     A.mu = (C)L.mu;
+    A.kappa = heat_coeff_host<C>(A.mu);
     A.forcing = (C)L.forcing;
     A.suth = (C)L.suth;
     A.flux = L.flux;

@@ -163,11 +163,28 @@ __device__ __forceinline__ C viscosity(C mu, C suth, const FaceState<C>& s) {
     }
 }
 
+// Heat-flux coefficient mu gamma / (Pr (gamma - 1)), in the reference's
+// operation order (device_functions.cuh:44). Constant viscosity: the value
+// formed once per launch on the host with the same IEEE operations
+// (kappa_const, heat_coeff_host); Sutherland's law: per point.
+template <class M, class C>
+__device__ __forceinline__ C heat_coeff(C mu, C kappa_const) {
+    if constexpr (!M::kSutherland)
+        return kappa_const;
+    else
+        return mu * Gas<C>::gamma() / (Gas<C>::pr() * Gas<C>::gm1());
+}
+
+template <class C>
+__host__ inline C heat_coeff_host(C mu) {
+    return mu * (C)1.4 / ((C)0.72 * ((C)1.4 - (C)1.0));
+}
+
 // Viscous flux along axis D at a face point from the state and the
 // 15-component conserved gradient g[3*var + axis] (only the 11 components
-// the D-flux reads are touched).
+// the D-flux reads are touched); kappa = heat_coeff(mu).
 template <int D, class C>
-__device__ __forceinline__ void viscous_flux(const FaceState<C>& s, C praw, const C* g, C mu, C* f) {
+__device__ __forceinline__ void viscous_flux(const FaceState<C>& s, C praw, const C* g, C mu, C kappa, C* f) {
     const C ir = s.ir;
     // d(vel_a)/d(x_b) for the pairs the D-flux needs
     auto dv = [&](int a, int b) -> C { return (g[3 * (1 + a) + b] - s.vel[a] * g[b]) * ir; };
@@ -183,7 +200,6 @@ __device__ __forceinline__ void viscous_flux(const FaceState<C>& s, C praw, cons
     C ke = (C)0.5 * (s.q[1] * s.vel[0] + s.q[2] * s.vel[1] + s.q[3] * s.vel[2]);
     C dke = (s.q[1] * g[3 + D] + s.q[2] * g[6 + D] + s.q[3] * g[9 + D]) * ir - ke * g[D] * ir;
     C dp = Gas<C>::gm1() * (g[12 + D] - dke);
-    C kappa = mu * Gas<C>::gamma() / (Gas<C>::pr() * Gas<C>::gm1());
     C heat = -kappa * (dp * ir - praw * g[D] * ir * ir);
     f[0] = (C)0.0;
     f[1] = tau[0];
@@ -196,7 +212,8 @@ __device__ __forceinline__ void viscous_flux(const FaceState<C>& s, C praw, cons
 // out[d][v] = F_euler,d - F_viscous,d. The velocity gradient, stress tensor
 // and heat flux are formed once and shared by the three directions.
 template <class C>
-__device__ __forceinline__ void volume_fluxes(const FaceState<C>& s, C praw, const C* g, C mu, C out[3][5]) {
+__device__ __forceinline__ void volume_fluxes(const FaceState<C>& s, C praw, const C* g, C mu, C kappa,
+                                              C out[3][5]) {
     const C ir = s.ir;
     C dvel[3][3];
 #pragma unroll
@@ -216,7 +233,6 @@ __device__ __forceinline__ void volume_fluxes(const FaceState<C>& s, C praw, con
         }
     }
     C ke = (C)0.5 * (s.q[1] * s.vel[0] + s.q[2] * s.vel[1] + s.q[3] * s.vel[2]);
-    C kappa = mu * Gas<C>::gamma() / (Gas<C>::pr() * Gas<C>::gm1());
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         C vn = s.vel[d];

@@ -328,6 +328,7 @@ struct StageAParams {
     P ra, rb, rc;
     C mu, forcing;
     C suth;             // Sutherland S = s_suth / t_ref, < 0: constant mu
+    C kappa;            // heat-flux coefficient of the constant mu (heat_coeff_host)
     int flags;
     int flux;           // scheme id, read when the kernel's FLUX is kFluxRuntime
     long long e0, e1;   // element range of this launch
@@ -436,7 +437,8 @@ __device__ __forceinline__ void viscous_face(const PA& A, SlotA<P, C>& sm, long 
                                              const C* fi) {
     const int f = 2 * D + side;
     C fv[NV];
-    viscous_flux<D>(s, praw, gt, viscosity<M>(A.mu, A.suth, s), fv);
+    const C mu = viscosity<M>(A.mu, A.suth, s);
+    viscous_flux<D>(s, praw, gt, mu, heat_coeff<M>(mu, A.kappa), fv);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         if constexpr (REG)
@@ -828,7 +830,8 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
             C praw;
             FaceState<C> s = make_face_state<M, C, P>(qp, praw);
             C F[3][NV];
-            volume_fluxes<C>(s, praw, g, viscosity<M>(A.mu, A.suth, s), F);
+            const C mu = viscosity<M>(A.mu, A.suth, s);
+            volume_fluxes<C>(s, praw, g, mu, heat_coeff<M>(mu, A.kappa), F);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 sm.g[v][p] = F[1][v];
