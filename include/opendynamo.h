@@ -421,10 +421,12 @@ int od_run(const od_params* p, const od_run_opts* o, od_run_result* r, char* err
 /* ------------------------------------------------------------------------
  * Ensembles (the batching form): independent boxes of uneven size, each with
  * its own extents, flux scheme, viscosity, forcing and time step, advanced
- * together in the f32 pipeline by ONE persistent cooperative launch per RK
- * stage (phase A of every box's elements, a grid barrier, phase B) or, in
- * the batched mode, two ordinary launches per stage over every box's tiles;
- * a step is replayed as a CUDA graph and the autotuner picks the mode. Each box agrees with advancing it alone with
+ * together in the f32 pipeline by ONE persistent launch per RK stage (phase
+ * A of every box's elements, a grid barrier, phase B; or, in the dynamic
+ * mode, tiles from a work queue with per-box phase-A counts instead of the
+ * barrier) or, in the batched mode, two ordinary launches per stage over
+ * every box's tiles; a step is replayed as a CUDA graph and the autotuner
+ * picks the mode. Each box agrees with advancing it alone with
  * od_step to f32 round-off (same stage code; a few values differ in the last
  * bit where the compiler contracts multiply-adds differently); results are
  * deterministic and do not depend on the grid size or the graph. No
@@ -462,13 +464,19 @@ int od_ensemble_step(od_ensemble* e, int n_steps);
 int od_ensemble_set_wait(od_ensemble* e, long long spin_limit, int extra_arrivals);
 
 /* Launch shape: elements per block (2 or 4; 16 threads each), blocks per SM
- * (<= 0: all that are co-resident), CUDA graph on/off. blocks_per_sm =
+ * (0: all that are co-resident), CUDA graph on/off. blocks_per_sm =
  * OD_ENSEMBLE_BATCHED selects the batched mode instead of the persistent
  * launch: two ordinary launches per stage over the tiles of every box (phase
  * A at 4 elements per block, elems_per_block ignored; phase B with a thread
  * per element, variable and x-line), no grid barrier; od_ensemble_info then
  * reports blocks_per_sm = OD_ENSEMBLE_BATCHED and grid = the phase-A blocks. */
 #define OD_ENSEMBLE_BATCHED (-1)
+/* blocks_per_sm = OD_ENSEMBLE_DYNAMIC: one persistent launch per stage whose
+ * blocks (all that are co-resident) take phase-A and phase-B tiles from a
+ * ticket queue; a phase-B tile waits (bounded, od_ensemble_set_wait) only
+ * for its own box's phase A, so there is no grid barrier. Up to 64 boxes;
+ * elems_per_block ignored (4). */
+#define OD_ENSEMBLE_DYNAMIC (-2)
 int od_ensemble_set_shape(od_ensemble* e, int elems_per_block, int blocks_per_sm, int use_graph);
 int od_ensemble_info(const od_ensemble* e, int* elems_per_block, int* blocks_per_sm, int* grid, int* graph);
 /* Autotuner: times every candidate shape for trial_steps steps on the

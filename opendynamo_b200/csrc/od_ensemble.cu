@@ -298,6 +298,77 @@ void* batched_a_ptr(bool fast, bool cp) {
 
 void* batched_b_ptr(bool cp) { return cp ? (void*)ensemble_b_kernel<true> : (void*)ensemble_b_kernel<false>; }
 
+// Dynamic persistent mode: ONE launch per stage whose blocks take work items
+// from a ticket counter in a fixed order: every box's phase-A tiles, and each
+// box's phase-B tiles placed at least a grid's worth of items after the box's
+// last phase-A tile. A phase-B tile waits (bounded) until its own box has
+// finished phase A, counted per box, so there is no grid-wide barrier and the
+// HBM-bound phase-B tiles of one box run on the same SMs as the issue-bound
+// phase-A tiles of the next. Every block takes tickets until it draws one
+// past the launch's items, so a launch consumes exactly items + grid tickets
+// and ticket / (items + grid) is the launch's index: the per-box counters
+// grow by the box's phase-A tile count per launch (targets need no reset
+// between launches or graph replays). Deadlock-free without co-residency: a
+// phase-B tile waits only for phase-A tiles that blocks already hold, and a
+// phase-A tile never waits. Per-box parameters from constant memory (up to
+// kConstBoxes boxes).
+constexpr int kDynEpb = 4;
+constexpr int kDynChunk = 4;   // tiles per work item (one ticket)
+
+template <class M>
+__global__ void __launch_bounds__(LPE * kDynEpb, 32 / kDynEpb)
+    ensemble_dyn_kernel(const int4* __restrict__ items, int total, const int* __restrict__ tiles_a,
+                        unsigned long long* adone, GridSync* sync) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int4 it;
+    __shared__ int skip;
+    const unsigned long long per = (unsigned long long)total + gridDim.x;
+    for (;;) {
+        __syncthreads();   // the previous item is done with the element slots and `it`
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(&sync->count, 1ull);
+            const unsigned long long item = t % per;
+            it = item < (unsigned long long)total ? items[item] : make_int4(-1, 0, 0, 0);
+            int bad = *(volatile int*)&sync->err;
+            if (!bad && it.x >= 0 && it.z == 1) {
+                // phase B of box it.x: wait for all its phase-A tiles of this launch
+                const unsigned long long target = (t / per + 1) * (unsigned long long)tiles_a[it.x] +
+                                                  (unsigned long long)max(sync->extra_arrivals, 0);
+                const long long limit = sync->spin_limit > 0 ? sync->spin_limit : kSpinLimit;
+                for (long long n = 0; ld_acquire(&adone[it.x]) < target; ++n) {
+                    if (n >= limit || *(volatile int*)&sync->err) {
+                        atomicExch(&sync->err, 1);
+                        bad = 1;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                __threadfence();
+            }
+            skip = bad;
+        }
+        __syncthreads();
+        const int4 w = it;
+        if (w.x < 0) break;   // past the launch's items (after an error too: tickets stay counted)
+        if (skip) continue;
+        if (w.z == 0) {
+            for (int k = 0; k < w.w; ++k) {
+                if (k) __syncthreads();   // the previous tile is done with the element slots
+                od::stage_a_tile<M, od::kFluxRuntime, kDynEpb>(c_boxes[w.x].A, smem_raw, w.y + k);
+            }
+            __threadfence();   // this thread's records and RHS before the box's count
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(&adone[w.x], (unsigned long long)w.w);
+        } else {
+            for (int k = 0; k < w.w; ++k) od::stage_b_tile<kDynEpb, true>(c_boxes[w.x].B, w.y + k);
+        }
+    }
+}
+
+void* dyn_ptr(bool fast) {
+    return fast ? (void*)ensemble_dyn_kernel<od::MathFast> : (void*)ensemble_dyn_kernel<od::MathIeee>;
+}
+
 template <class M, int EPB>
 void* kernel_ptr(bool cp) {
     return cp ? (void*)ensemble_stage_kernel<M, EPB, true> : (void*)ensemble_stage_kernel<M, EPB, false>;
@@ -329,10 +400,15 @@ struct od_ensemble {
     int2* d_tile_map = nullptr;      // (box, tile in box) of every phase-A tile (sized for 2 elements per tile)
     int2* d_tile_map_b = nullptr;    // the same for the phase-B tiles
     GridSync* d_sync = nullptr;
-    // shape; batched: two ordinary launches per stage instead of the persistent one
+    // shape; batched: two ordinary launches per stage instead of the persistent one;
+    // dynamic: one launch per stage, work items and per-box phase-A counts
     int epb = 4, bps = 0, grid = 0;
-    bool batched = false;
+    bool batched = false, dynamic = false;
     long long tiles_a = 0, tiles_b = 0;
+    int4* d_items = nullptr;            // dynamic mode: (box, first tile, phase, tiles) in issue order
+    int n_items = 0;
+    int* d_tiles_box = nullptr;         // phase-A tiles per box
+    unsigned long long* d_adone = nullptr;   // phase-A tiles done per box (monotonic)
     bool use_graph = true, graph_ok = false;
     cudaGraphExec_t exec = nullptr;
     std::string err;
@@ -371,6 +447,42 @@ int build_stage_params(od_ensemble* E) {
     }
     E->tiles_a = sa[nb];
     E->tiles_b = sb[nb];
+    if (E->dynamic) {
+        // issue order: phase-A tiles box by box; a box's phase-B tiles once at
+        // least a grid's worth of phase-A items follow its last phase-A tile
+        std::vector<int4> items;
+        items.reserve((size_t)(sa[nb] + sb[nb]));
+        std::vector<std::pair<int, long long>> pending;   // (box, phase-A items issued when it ended)
+        size_t head = 0;
+        long long na = 0;
+        // an item: (box, first tile, phase, tiles), up to kDynChunk tiles of one box and phase
+        auto emit_b = [&](int b) {
+            const long long n = sb[b + 1] - sb[b];
+            for (long long t = 0; t < n; t += kDynChunk)
+                items.push_back(make_int4(b, (int)t, 1, (int)std::min<long long>(kDynChunk, n - t)));
+        };
+        std::vector<int> tiles_box(nb);
+        for (int b = 0; b < nb; ++b) {
+            const long long n = sa[b + 1] - sa[b];
+            tiles_box[b] = (int)n;
+            for (long long t = 0; t < n; t += kDynChunk) {
+                items.push_back(make_int4(b, (int)t, 0, (int)std::min<long long>(kDynChunk, n - t)));
+                ++na;
+                while (head < pending.size() && na - pending[head].second >= E->grid) emit_b(pending[head++].first);
+            }
+            pending.push_back({b, na});
+        }
+        while (head < pending.size()) emit_b(pending[head++].first);
+        if (E->d_items) cudaFree(E->d_items);
+        E->d_items = nullptr;
+        E->n_items = (int)items.size();
+        cudaError_t c = cudaMalloc(&E->d_items, sizeof(int4) * items.size());
+        if (c == cudaSuccess)
+            c = cudaMemcpy(E->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
+        if (c == cudaSuccess)
+            c = cudaMemcpy(E->d_tiles_box, tiles_box.data(), sizeof(int) * nb, cudaMemcpyHostToDevice);
+        if (c != cudaSuccess) return ecuda(E, c, "dynamic work items");
+    }
     for (int s = 0; s < 3; ++s) {
         for (int b = 0; b < nb; ++b) {
             const od_box& x = E->box[b];
@@ -452,6 +564,12 @@ cudaError_t launch_stage(od_ensemble* E, int s) {
                                                 cudaMemcpyDeviceToDevice, E->stream);
         if (c != cudaSuccess) return c;
     }
+    if (E->dynamic) {
+        void* args[] = {(void*)&E->d_items, (void*)&E->n_items, (void*)&E->d_tiles_box, (void*)&E->d_adone,
+                        (void*)&E->d_sync};
+        return cudaLaunchKernel(dyn_ptr(E->fast), dim3((unsigned)E->grid), dim3(LPE * kDynEpb), args,
+                                dyn_smem(kDynEpb), E->stream);
+    }
     if (E->batched) {
         void* args_a[] = {(void*)&E->d_stage[s], (void*)&E->d_tile_map};
         cudaError_t c = cudaLaunchKernel(batched_a_ptr(E->fast, cp), dim3((unsigned)E->tiles_a),
@@ -489,29 +607,37 @@ void drop_graph(od_ensemble* E) {
 // elements per block)
 int apply_shape(od_ensemble* E, int epb, int bps, bool use_graph) {
     const bool batched = bps == OD_ENSEMBLE_BATCHED;
+    const bool dynamic = bps == OD_ENSEMBLE_DYNAMIC;
     if (batched) epb = kBatchEpbA;
+    if (dynamic) epb = kDynEpb;
+    if (bps < 0 && !batched && !dynamic) return efail(E, OD_ERR_ARG, "unknown launch mode");
     if (epb != 2 && epb != 4) return efail(E, OD_ERR_ARG, "elements per block must be 2 or 4");
     const bool cp = E->box.size() <= (size_t)kConstBoxes;
-    void* fn = batched ? batched_a_ptr(E->fast, cp) : pick_kernel(E->fast, epb, cp);
+    if (dynamic && !cp) return efail(E, OD_ERR_ARG, "the dynamic mode takes at most 64 boxes");
+    void* fn = dynamic ? dyn_ptr(E->fast) : batched ? batched_a_ptr(E->fast, cp) : pick_kernel(E->fast, epb, cp);
     cudaError_t c = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem(epb));
     if (c != cudaSuccess) return ecuda(E, c, "cudaFuncSetAttribute");
     int maxb = 0;
     c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, fn, LPE * epb, dyn_smem(epb));
     if (c != cudaSuccess) return ecuda(E, c, "occupancy");
     if (maxb <= 0) return efail(E, OD_ERR_CUDA, "ensemble kernel cannot be resident");
-    if (!batched && (bps <= 0 || bps > maxb)) bps = maxb;
+    if (dynamic || (!batched && (bps <= 0 || bps > maxb))) bps = maxb;
     drop_graph(E);
-    const bool rebuild = epb != E->epb || batched != E->batched || !E->d_stage[0];
+    const bool rebuild = epb != E->epb || batched != E->batched || dynamic != E->dynamic || dynamic ||
+                         !E->d_stage[0];
     E->epb = epb;
     E->batched = batched;
+    E->dynamic = dynamic;
     E->use_graph = use_graph;
+    E->grid = bps * E->nsm;   // the dynamic mode's item order depends on it
     if (rebuild) {
         if (int rc = build_stage_params(E)) return rc;
     }
-    E->bps = batched ? OD_ENSEMBLE_BATCHED : bps;
-    E->grid = batched ? (int)E->tiles_a : bps * E->nsm;
-    // a new grid size restarts the arrival counter
+    E->bps = batched ? OD_ENSEMBLE_BATCHED : dynamic ? OD_ENSEMBLE_DYNAMIC : bps;
+    if (batched) E->grid = (int)E->tiles_a;
+    // a new grid size restarts the arrival / ticket counter and the per-box counts
     c = cudaMemsetAsync(E->d_sync, 0, sizeof(GridSync), E->stream);
+    if (c == cudaSuccess) c = cudaMemsetAsync(E->d_adone, 0, sizeof(unsigned long long) * E->box.size(), E->stream);
     if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
     if (c != cudaSuccess) return ecuda(E, c, "barrier reset");
     if (use_graph) {
@@ -556,7 +682,9 @@ int check_sync_flag(od_ensemble* E) {
     cudaError_t c = cudaMemcpyAsync(&h, E->d_sync, sizeof h, cudaMemcpyDeviceToHost, E->stream);
     if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
     if (c != cudaSuccess) return ecuda(E, c, "ensemble step");
-    if (h.err) return efail(E, OD_ERR_CUDA, "ensemble grid barrier timed out (blocks not co-resident)");
+    if (h.err)
+        return efail(E, OD_ERR_CUDA, E->dynamic ? "ensemble phase-B wait timed out (a box's phase A never completed)"
+                                                : "ensemble grid barrier timed out (blocks not co-resident)");
     return OD_OK;
 }
 
@@ -606,6 +734,8 @@ int od_ensemble_create(const od_box* boxes, int nbox, int device, int fast_math,
     if (c == cudaSuccess) c = cudaMalloc(&E->d_tile_map, sizeof(int2) * (size_t)max_tiles);
     if (c == cudaSuccess) c = cudaMalloc(&E->d_tile_map_b, sizeof(int2) * (size_t)max_tiles);
     if (c == cudaSuccess) c = cudaMalloc(&E->d_sync, sizeof(GridSync));
+    if (c == cudaSuccess) c = cudaMalloc(&E->d_tiles_box, sizeof(int) * nbox);
+    if (c == cudaSuccess) c = cudaMalloc(&E->d_adone, sizeof(unsigned long long) * nbox);
     if (c != cudaSuccess) {
         *out = E;
         return ecuda(E, c, "allocation");
@@ -634,6 +764,9 @@ void od_ensemble_destroy(od_ensemble* E) {
     if (E->d_tile_map) cudaFree(E->d_tile_map);
     if (E->d_tile_map_b) cudaFree(E->d_tile_map_b);
     if (E->d_sync) cudaFree(E->d_sync);
+    if (E->d_items) cudaFree(E->d_items);
+    if (E->d_tiles_box) cudaFree(E->d_tiles_box);
+    if (E->d_adone) cudaFree(E->d_adone);
     if (E->pool) cudaFree(E->pool);
     if (E->stream) cudaStreamDestroy(E->stream);
     delete E;
@@ -677,8 +810,10 @@ int od_ensemble_set_wait(od_ensemble* E, long long spin_limit, int extra_arrival
     GridSync h{};
     h.spin_limit = spin_limit;
     h.extra_arrivals = extra_arrivals;
-    // restarts the arrival counter and clears a timed-out barrier's error flag
+    // restarts the arrival / ticket counter and the per-box counts and clears
+    // a timed-out wait's error flag
     cudaError_t c = cudaMemcpyAsync(E->d_sync, &h, sizeof h, cudaMemcpyHostToDevice, E->stream);
+    if (c == cudaSuccess) c = cudaMemsetAsync(E->d_adone, 0, sizeof(unsigned long long) * E->box.size(), E->stream);
     if (c == cudaSuccess) c = cudaStreamSynchronize(E->stream);
     if (c != cudaSuccess) return ecuda(E, c, "od_ensemble_set_wait");
     return OD_OK;
@@ -733,6 +868,7 @@ int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t r
         std::vector<int> cands;
         for (int b = maxb; b >= 1; b = b > 2 ? b * 3 / 4 : b - 1) cands.push_back(b);
         if (epb == kBatchEpbA) cands.insert(cands.begin(), OD_ENSEMBLE_BATCHED);
+        if (epb == kDynEpb && E->box.size() <= (size_t)kConstBoxes) cands.insert(cands.begin(), OD_ENSEMBLE_DYNAMIC);
         for (int bps : cands) {
             if ((rc = apply_shape(E, epb, bps, true))) break;
             if ((rc = enqueue_steps(E, 1))) break;
@@ -743,7 +879,10 @@ int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t r
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
             char line[128];
-            if (E->batched)
+            if (E->dynamic)
+                std::snprintf(line, sizeof line, "dynamic (one launch per stage, %d items, grid %d) graph=%d: %.4f ms/step\n",
+                              E->n_items, E->grid, E->graph_ok ? 1 : 0, ms / trial_steps);
+            else if (E->batched)
                 std::snprintf(line, sizeof line, "batched (two launches per stage, %lld + %lld blocks) graph=%d: %.4f ms/step\n",
                               E->tiles_a, E->tiles_b, E->graph_ok ? 1 : 0, ms / trial_steps);
             else
@@ -775,6 +914,8 @@ int od_ensemble_autotune(od_ensemble* E, int trial_steps, char* report, size_t r
     char line[128];
     if (best_bps == OD_ENSEMBLE_BATCHED)
         std::snprintf(line, sizeof line, "chosen: batched\n");
+    else if (best_bps == OD_ENSEMBLE_DYNAMIC)
+        std::snprintf(line, sizeof line, "chosen: dynamic\n");
     else
         std::snprintf(line, sizeof line, "chosen: epb=%d blocks/SM=%d\n", best_epb, best_bps);
     rep += line;

@@ -81,6 +81,9 @@ def benchmark_boxes(count=64, seed=7, n_min=8, n_max=32, cfl=0.3) -> list[Box]:
 # blocks_per_sm of set_shape / info for the batched mode: two ordinary
 # launches per stage instead of the persistent one (OD_ENSEMBLE_BATCHED)
 BATCHED = -1
+# ... and for the dynamic persistent mode: one launch per stage, work queue,
+# per-box phase-A counts instead of a grid barrier (OD_ENSEMBLE_DYNAMIC)
+DYNAMIC = -2
 
 
 class Ensemble:
@@ -145,7 +148,8 @@ class Ensemble:
 
     def set_shape(self, elems_per_block: int, blocks_per_sm: int = 0, graph: bool = True):
         """Persistent launch shape (blocks_per_sm 0: all co-resident), or
-        blocks_per_sm = BATCHED for two launches per stage."""
+        blocks_per_sm = BATCHED for two launches per stage, DYNAMIC for the
+        work-queue persistent launch."""
         self._chk(self._lib.od_ensemble_set_shape(self._h, elems_per_block, blocks_per_sm, int(graph)),
                   "od_ensemble_set_shape")
 

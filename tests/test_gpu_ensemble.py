@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from helpers import random_smooth
-from opendynamo_b200.forms.ensemble import BATCHED, Box, Ensemble, benchmark_boxes
+from opendynamo_b200.forms.ensemble import BATCHED, DYNAMIC, Box, Ensemble, benchmark_boxes
 from opendynamo_b200.solver import Solver
 
 BOXES = [
@@ -119,6 +119,35 @@ def test_batched_mode_equals_boxes_alone(graph):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("graph", [True, False])
+def test_dynamic_mode_equals_boxes_alone(graph):
+    """One launch per stage with a work queue and per-box phase-A counts: the
+    same per-box results as the batched launches (the same tile code),
+    deterministic, and its ticket accounting holds over many launches."""
+    states = _states(BOXES)
+    want = _alone(BOXES, states, 5)
+    with Ensemble(BOXES) as E:
+        E.set_shape(4, BATCHED, graph)
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.step(5)
+        batched = [E.get_state(k) for k in range(len(BOXES))]
+        E.set_shape(2, DYNAMIC, graph)
+        info = E.info()
+        assert info["blocks_per_sm"] == DYNAMIC and info["elems_per_block"] == 4 and info["grid"] > 0
+        runs = []
+        for _ in range(2):
+            for k, u in enumerate(states):
+                E.set_state(k, u)
+            E.step(5)
+            runs.append([E.get_state(k) for k in range(len(BOXES))])
+    for k in range(len(BOXES)):
+        _close(runs[0][k], want[k])
+        _close(runs[0][k], batched[k])
+        assert runs[1][k].tobytes() == runs[0][k].tobytes(), k
+
+
+@pytest.mark.gpu
 def test_autotune_and_benchmark_boxes():
     boxes = benchmark_boxes(count=6, n_min=2, n_max=5)
     assert len({b.flux for b in boxes}) >= 1 and all(2 <= b.n[0] <= 5 for b in boxes)
@@ -128,7 +157,7 @@ def test_autotune_and_benchmark_boxes():
         for k, u in enumerate(states):
             E.set_state(k, u)
         rep = E.autotune(trial_steps=1)
-        assert "chosen:" in rep and "ms/step" in rep and "batched" in rep
+        assert "chosen:" in rep and "ms/step" in rep and "batched" in rep and "dynamic" in rep
         # the autotuner restores the states it stepped
         for k, u in enumerate(states):
             assert E.get_state(k).tobytes() == u.tobytes()
@@ -171,6 +200,34 @@ def test_barrier_timeout_is_reported_and_recoverable(graph):
         # the flag is sticky until cleared
         with pytest.raises(N.OdError, match="grid barrier timed out"):
             E.step(1)
+        E.set_wait(0, 0)
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.step(2)
+        for k in range(len(BOXES)):
+            _close(E.get_state(k), want[k])
+
+
+@pytest.mark.gpu
+def test_dynamic_mode_wait_timeout_is_reported_and_recoverable():
+    """The dynamic mode's bounded phase-B wait: with every box's phase-A
+    target raised by one tile (nothing reaches it) and a short poll limit,
+    the first phase-B tile gives up and sets the error flag, the other
+    blocks skip their items; od_ensemble_step reports OD_ERR_CUDA; after
+    od_ensemble_set_wait(0, 0) the same ensemble steps correctly again."""
+    import time
+    from opendynamo_b200 import _native as N
+    states = _states(BOXES)
+    want = _alone(BOXES, states, 2)
+    with Ensemble(BOXES) as E:
+        E.set_shape(4, DYNAMIC, True)
+        for k, u in enumerate(states):
+            E.set_state(k, u)
+        E.set_wait(spin_limit=20000, extra_arrivals=1)
+        t0 = time.perf_counter()
+        with pytest.raises(N.OdError, match="phase-B wait timed out"):
+            E.step(2)
+        assert time.perf_counter() - t0 < 30.0
         E.set_wait(0, 0)
         for k, u in enumerate(states):
             E.set_state(k, u)
