@@ -345,8 +345,9 @@ def run_precision_form(args, world, rank, local):
 
 
 def run_ensemble_form(args, world, rank, local):
-    """Batching form: the 64-box ensemble (seed 7) in one persistent launch
-    per RK stage (autotuned, CUDA graph) against looping single instances."""
+    """Batching form: the 64-box ensemble (seed 7) in the autotuner's mode
+    (two batched launches per RK stage, or one persistent launch with a grid
+    barrier or a work queue; CUDA graph) against looping single instances."""
     if rank != 0:
         return None
     import torch

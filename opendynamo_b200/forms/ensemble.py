@@ -1,7 +1,9 @@
-"""Batching form: ensembles of independent boxes of uneven size advanced by
-one persistent launch per RK stage (``od_ensemble_*`` in libopendynamo),
-plus the benchmark ensemble (64 Taylor-Green / tripped-channel boxes drawn
-from seed 7) and its comparison against looping single instances.
+"""Batching form: ensembles of independent boxes of uneven size advanced
+together (``od_ensemble_*`` in libopendynamo): two batched launches per RK
+stage, or one persistent launch per stage with a grid barrier or a work
+queue, picked by the autotuner; plus the benchmark ensemble (64
+Taylor-Green / tripped-channel boxes drawn from seed 7) and its comparison
+against looping single instances.
 """
 
 from __future__ import annotations
