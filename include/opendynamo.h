@@ -341,7 +341,8 @@ typedef struct od_ic_params {
  * amplitude, not the script's bits. Taylor-Green (double, on [0,lx]x[0,ly]x
  * [0,lz]): u = v0 sin x cos y cos z, v = -v0 cos x sin y cos z, w = 0,
  * rho = 1, p = 1/1.4 + v0^2/16 (cos 2x + cos 2y)(cos 2z + 2).
- * Replaces: initial_condition / apply_trip of scripts/make_initial_state.py. */
+ * Replaces: initial_condition / apply_trip of scripts/make_initial_state.py
+ * (:122-241). */
 int od_make_initial_state(const od_ic_params* p, void* planes, size_t bytes, int u_f64);
 
 /* ------------------------------------------------------------------------
