@@ -50,7 +50,8 @@ def variants():
         out.append((prec, prec, prec, prec, flux, wall, True))
     out.append(("f64", "f32", "f32", "f32", "slau2", True, True))    # constants.cuh defaults
     out.append(("f64", "f32", "f32", "f64", "slau2", True, True))    # f64 compute, f32 Q / RHS
-    out.append(("f32", "f32", "f32", "f32", "slau2", True, False))   # strict IEEE f32
+    for flux in FLUX_MACRO:                                            # strict IEEE f32, every flux
+        out.append(("f32", "f32", "f32", "f32", flux, True, False))
     return out
 
 

@@ -76,25 +76,27 @@ def test_tgv_f64_100_steps_vs_extended_precision():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mesh", [(12, 8, 6), (48, 48, 48)])
-def test_channel_f32_100_steps_vs_reference(mesh):
-    """Config 2 physics (channel, SLAU2, y walls, f32, the reference's
-    fast-math build): 100 steps from the same IC. The f64 truth is this
-    project's f64 pipeline (itself held to 1e-10 of the reference's f64)."""
+@pytest.mark.parametrize("mesh,flux", [((12, 8, 6), "slau2"), ((12, 8, 6), "ausm+"), ((12, 8, 6), "rusanov"),
+                                       ((48, 48, 48), "slau2")])
+def test_channel_f32_100_steps_vs_reference(mesh, flux):
+    """Config 2 physics (channel, y walls, f32, the reference's fast-math
+    build; SLAU2 at 48^3, every flux at 12x8x6): 100 steps from the same IC.
+    The f64 truth is this project's f64 pipeline (itself held to 1e-10 of the
+    reference's f64)."""
     u = channel_trip(*mesh, amp=0.01, dtype=np.float32)
     dt = 2e-4
     runs = {}
     for name, fm, u_start in (("ref", True, u), ("ref_ulp", True, ulp_perturbed(u)), ("ref_ieee", False, u)):
-        with _ref()(*mesh, *BOX, "slau2", True, "f32", fast_math=fm) as r:
+        with _ref()(*mesh, *BOX, flux, True, "f32", fast_math=fm) as r:
             r.set_state(u_start)
             r.step(100, dt)
             runs[name] = r.get_state()
     ref = runs["ref"]
-    with Solver(make_params(*mesh, *BOX, "slau2", True, "f32")) as s:
+    with Solver(make_params(*mesh, *BOX, flux, True, "f32")) as s:
         s.set_state(u)
         s.step(100, float(np.float32(dt)))
         got = s.get_state()
-    with Solver(make_params(*mesh, *BOX, "slau2", True, "f64")) as s:
+    with Solver(make_params(*mesh, *BOX, flux, True, "f64")) as s:
         s.set_state(u.astype(np.float64))
         s.step(100, float(np.float32(dt)))
         truth = s.get_state()
@@ -103,7 +105,7 @@ def test_channel_f32_100_steps_vs_reference(mesh):
     table = {"pair (ours vs reference)": rel_l2(got, ref), "reference vs itself from +-1 ulp": spread,
              "reference fast-math vs IEEE": fm_ieee, "ours vs f64": rel_l2(got, truth),
              "reference vs f64": rel_l2(ref, truth)}
-    print(f"\nf32 parity table, channel {mesh}, 100 steps (rho, rho*u, rho*v, rho*w, E):")
+    print(f"\nf32 parity table, channel {mesh}, {flux}, 100 steps (rho, rho*u, rho*v, rho*w, E):")
     for k, v in table.items():
         print(f"  {k:34s} " + " ".join(f"{x:9.2e}" for x in v))
     assert_f32_parity(got, ref, truth, spread)
