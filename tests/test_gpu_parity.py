@@ -88,7 +88,7 @@ def test_tgv_f64_100_steps():
 @pytest.mark.parametrize("flux", ["slau2", "rusanov"])
 def test_channel_f32_100_steps(flux):
     """f32 pipeline, channel with walls, 100 steps: against the oracle's f32
-    restatement, judged with the f64 oracle run as the truth."""
+    restatement, measured against the f64 oracle run as the truth."""
     mesh = (4, 4, 3)
     u = channel_trip(*mesh, amp=0.01, dtype=np.float32)
     op, dp = _pair(mesh, flux, True, "f32")
