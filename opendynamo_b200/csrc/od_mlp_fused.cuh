@@ -9,7 +9,7 @@
 // Only the features (layer 1's A, written in this kernel's tile layout by
 // the features kernel) and the weights (every layer's B, from a step-ordered
 // image in the shared-memory layout, tile_fused_weights) are streamed, in
-// 64-wide K blocks, three stages deep, as bulk copies that complete on the
+// 64-wide K blocks, four stages deep, as bulk copies that complete on the
 // stage's `full` mbarrier. Thread 0 alone runs the K loop: it issues the
 // copies and tcgen05.mma (kind::f16, M = 128, K = 16) and commits each stage's
 // MMAs to its `bar` mbarrier; the 16 warps meet at the end of every layer for
@@ -17,9 +17,9 @@
 // output layer runs as two passes of N = 160 (columns 0-159 and 160-319:
 // variables 0-2.5 and 2.5-5).
 //
-// Shared memory (200 KB): one 64 KB activation buffer of four 128 x 64
-// k-blocks, three 32 KB weight stages, a 34 KB staging area for the RHS
-// update and the biases. A layer's epilogue overwrites its own input in
+// Shared memory (197 KB): one 64 KB activation buffer of four 128 x 64
+// k-blocks, four 32 KB weight stages and the biases (the RHS update reduces
+// straight from registers). A layer's epilogue overwrites its own input in
 // place: it starts only after all of the layer's MMAs have completed. During
 // layer 1 the activation buffer holds the feature stages instead (layer 1's
 // output is written after its last MMA). Tensor memory: 256 fp32 columns,
@@ -34,7 +34,7 @@ namespace od {
 namespace mlp {
 
 constexpr int kFIn = 896, kFHid = 256, kFOut = 320, kFPass = 160;
-constexpr int kFStages = 3;
+constexpr int kFStages = 4;
 constexpr int kFThreads = 512;   // 16 warps: warp w reads TMEM lanes 32 (w % 4) .. +31, column group w / 4
 constexpr int kFGroups = kFThreads / 128;   // column groups of the epilogues
 constexpr int kFSteps = kFIn / BK + 2 * (kFHid / BK) + 2 * (kFHid / BK);   // 14 + 4 + 4 + 2 x 4 = 30
@@ -45,7 +45,6 @@ static_assert(22 * kFStageBytes + 8 * kFOutStageBytes == kFusedWeightBytes, "wei
 struct FusedSmem {
     alignas(1024) unsigned char h[4][BM * BK * 2];   // activations [k-block]; layer 1: feature stages
     alignas(1024) unsigned char b[kFStages][kFHid * BK * 2];   // weight stages
-    alignas(16) float stg[kFThreads / 32][32 * 17];   // per-warp 32 x 16 staging tile (row stride 17)
     alignas(16) float bias[3 * kFHid + kFOut];   // the four layers' biases, read by every epilogue
     alignas(8) unsigned long long bar[kFStages];    // the stage's MMAs are complete (stage free)
     alignas(8) unsigned long long full[kFStages];   // the stage's weight tile has landed
@@ -156,38 +155,35 @@ __device__ __forceinline__ void fused_hidden_epilogue(const FusedArgs& g, FusedS
 }
 
 // Epilogue of output pass p: rhs[var][row*64 + point] += scale[var] * (C + bias)
-// for the columns var*64 + point of this pass; 16 columns at a time through
-// the warp's staging tile, so that every reduction instruction covers two
-// contiguous 64-byte row segments.
+// for the columns var*64 + point of this pass. Each thread owns one row (its
+// TMEM lane) and 32 consecutive columns, 32 consecutive RHS values: eight
+// 16-byte vector reductions, one contribution per RHS value (the same
+// rounding as load + add + store, without the load's round trip), and no
+// staging tile, so that the shared memory holds four weight stages.
 __device__ __forceinline__ void fused_out_epilogue(const FusedArgs& g, FusedSmem& sm, int pass, uint32_t tmem,
                                                    int m0) {
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, quarter = warp & 3, grp = warp >> 2;
     const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
-    float* stg = sm.stg[warp];
-    const int row0 = m0 + quarter * 32;
-    const int sub = lane >> 4, col = lane & 15;
+    const int row = m0 + quarter * 32 + lane;
 #pragma unroll 1
     for (int c0 = grp * 32; c0 < kFPass; c0 += 32 * kFGroups) {   // 32-column chunks, round robin over the groups
         float v[32];
-        fused_tmem_ld32(lane_base, c0, v);
-        const int n = pass * kFPass + c0;   // 32 columns inside one variable's 64-point block
+        fused_tmem_ld32(lane_base, c0, v);   // warp-collective: every lane takes part
+        const int n = pass * kFPass + c0;    // 32 columns inside one variable's 64-point block
         const int var = n >> 6;
         const float sc = var == 0 ? g.rhs_scale[0] : var == 1 ? g.rhs_scale[1] : var == 2 ? g.rhs_scale[2]
                        : var == 3 ? g.rhs_scale[3] : g.rhs_scale[4];
+        if (row >= g.rhs_rows) continue;
+        float* base = g.rhs + (size_t)var * g.rhs_npts + (size_t)row * 64 + (n & 63);
 #pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-#pragma unroll
-            for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = v[16 * hh + j] + sm.bias[3 * kFHid + n + 16 * hh + j];
-            __syncwarp();
-            float* base = g.rhs + (size_t)var * g.rhs_npts + (n & 63) + 16 * hh + col;
-            // one reduction per RHS value (a single contribution each: the same
-            // rounding as load + add + store, without the load's round trip)
-#pragma unroll
-            for (int rr = 0; rr < 32; rr += 2) {
-                const int r = rr + sub;
-                if (row0 + r < g.rhs_rows) atomicAdd(base + (size_t)(row0 + r) * 64, sc * stg[r * 17 + col]);
-            }
-            __syncwarp();
+        for (int q = 0; q < 8; ++q) {
+            const float a0 = sc * (v[4 * q] + sm.bias[3 * kFHid + n + 4 * q]);
+            const float a1 = sc * (v[4 * q + 1] + sm.bias[3 * kFHid + n + 4 * q + 1]);
+            const float a2 = sc * (v[4 * q + 2] + sm.bias[3 * kFHid + n + 4 * q + 2]);
+            const float a3 = sc * (v[4 * q + 3] + sm.bias[3 * kFHid + n + 4 * q + 3]);
+            asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(base + 4 * q), "f"(a0), "f"(a1),
+                         "f"(a2), "f"(a3)
+                         : "memory");
         }
     }
 }
