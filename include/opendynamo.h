@@ -539,7 +539,8 @@ int od_mlp_set_scaling(od_mlp* m, const float* mean14, const float* scale14, con
  * Results agree to bf16 round-off of the same operands. */
 int od_mlp_set_fused(od_mlp* m, int on);
 /* Attach (m != null) or detach the network to a solver: every RK stage of
- * od_step then runs phase A, features of the stage's state, the network,
+ * od_step then runs phase A, features of the stage's state (written by phase
+ * A itself for the fused network with constant viscosity), the network,
  * rhs += out_scale * output, phase B. Needs an f32 state. The network must
  * outlive the attachment. */
 int od_attach_closure(od_ctx* ctx, od_mlp* m);

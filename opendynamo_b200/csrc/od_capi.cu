@@ -255,15 +255,24 @@ int enqueue_stage(od_ctx* c, const void* u_in, const void* u0, void* u_out, doub
     }
     const int K = c->slabs;
     if (c->hook) {
-        // phase A leaves the RHS in c->rhs; the hook corrects it; phase B finishes the stage
+        // phase A leaves the RHS in c->rhs (and, f32 state with constant
+        // viscosity, writes the closure's features); the hook corrects the
+        // RHS; phase B finishes the stage
         L.e0 = 0;
         L.e1 = c->nelem;
         L.phases = 1;
         L.ev[0] = tev[0];
         L.ev[1] = tev[1];
         L.ev[2] = nullptr;
+        od::StageFeatures sf;
+        const bool feat = c->combo == od::kF32 && c->p.viscosity_model == OD_VISC_CONSTANT &&
+                          od::closure_stage_features(c->hook_user, &sf);
+        L.feat = feat ? &sf : nullptr;
         cudaError_t e = c->fns.launch(L, c->stream);
-        if (e == cudaSuccess) e = c->hook(c->hook_user, u_in, c->rhs, c->stream);
+        L.feat = nullptr;
+        if (e == cudaSuccess)
+            e = feat ? od::closure_network_hook(c->hook_user, u_in, c->rhs, c->stream)
+                     : c->hook(c->hook_user, u_in, c->rhs, c->stream);
         if (e == cudaSuccess) {
             L.phases = 2;
             L.ev[0] = L.ev[1] = nullptr;

@@ -770,8 +770,40 @@ int od_f32_to_bf16(const float* a, void* b, long long n, void* stream) {
 // ------------------------------------------------------------------ solver hook
 // Between phase A (which leaves the RHS in the solver's RHS buffer) and
 // phase B of every RK stage: features of the stage's input state, network
-// forward, rhs += out_scale * output.
+// forward, rhs += out_scale * output. With the fused network on an f32
+// state, phase A writes the features itself (closure_stage_features) and
+// closure_network_hook runs the network alone.
 namespace od {
+static_assert(kChan == kFeatChan && kClip == kFeatClip, "phase A writes the same features");
+
+bool closure_stage_features(void* user, StageFeatures* out) {
+    od_mlp* m = (od_mlp*)user;
+    if (!m || !m->fused || m->attached_f64 || !m->Xc) return false;
+    out->X = m->Xc;
+    for (int d = 0; d < 3; ++d) out->jac[d] = m->fp.jac[d];
+    for (int a = 0; a < 16; ++a) out->D[a] = m->fp.D[a];
+    for (int c = 0; c < kChan; ++c) {
+        out->mean[c] = m->fp.mean[c];
+        out->inv_scale[c] = m->fp.inv_scale[c];
+    }
+    return true;
+}
+
+cudaError_t closure_network_hook(void* user, const void* u_in, void* rhs, cudaStream_t s) {
+    (void)u_in;
+    od_mlp* m = (od_mlp*)user;
+    od::mlp::FusedArgs a{};
+    a.X = m->Xc;
+    a.Wt = m->wt;
+    for (int l = 0; l < 4; ++l) a.bias[l] = m->w + m->off_b[l];
+    a.rhs = (float*)rhs;
+    a.rhs_npts = m->nelem_c * 64;
+    a.rhs_rows = (int)m->nelem_c;
+    for (int v = 0; v < 5; ++v) a.rhs_scale[v] = m->out_scale[v];
+    a.err = m->err;
+    return od::mlp::launch_fused(a, (int)m->mpad_c, s);
+}
+
 cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStream_t s) {
     od_mlp* m = (od_mlp*)user;
     cudaError_t e = cudaSuccess;

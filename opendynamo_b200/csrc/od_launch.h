@@ -27,12 +27,29 @@ struct TablesD {
     double pts[4], D[16], eL[4], eR[4], gL[4], gR[4];
 };
 
+// The learned closure's input, written by phase A when the closure is
+// attached (f32 state, constant viscosity): each element's 14 channels x 64
+// points as bf16 in the fused inference kernel's tile layout, with the
+// features kernel's parameters and operation order. Channels: rho, rho*u,
+// rho*v, rho*w, E and d(u_a)/d(x_b); standardised inputs are clipped to
+// +-kFeatClip.
+constexpr int kFeatChan = 14;
+constexpr float kFeatClip = 8.0f;
+
+struct StageFeatures {
+    void* X;              // bf16 tiles: [element / 128][channel][128 x 64 core-matrix layout]
+    float jac[3];
+    float D[16];
+    float mean[kFeatChan], inv_scale[kFeatChan];
+};
+
 struct StageLaunch {
     const void* u_in;
     const void* u0;      // null on stage 1 / single RHS evaluations
     void* u_out;
     void* fv;            // face-flux scratch (kFaceWords per element)
     void* rhs;           // RHS buffer of the deferred RK combination (null otherwise)
+    const StageFeatures* feat;   // phase A also writes the closure's features (null otherwise)
     int nx, ny, nz, y_wall;
     long long nelem;
     TablesD tab;
@@ -68,8 +85,13 @@ struct od_mlp;
 
 namespace od {
 
-// the learned closure's hook and its per-mesh preparation (od_closure.cu)
+// the learned closure's hook and its per-mesh preparation (od_closure.cu);
+// closure_stage_features fills the parameters for phase A to write the
+// features itself (false: the hook computes them), closure_network_hook then
+// runs the network alone
 cudaError_t closure_stage_hook(void* user, const void* u_in, void* rhs, cudaStream_t s);
+bool closure_stage_features(void* user, StageFeatures* out);
+cudaError_t closure_network_hook(void* user, const void* u_in, void* rhs, cudaStream_t s);
 int closure_prepare(od_mlp* m, int nx, int ny, int nz, double lx, double ly, double lz, bool f64);
 
 // Diagnostics (od_diag.cu): accumulates into d_vol6 / d_prof (zeroed by the caller).

@@ -20,25 +20,42 @@ Tab<T> cast_tab(const TablesD& t) {
     return r;
 }
 
+// The kernels that also write the closure's features exist for the all-f32
+// pipeline with constant viscosity at 4 elements per block (the closure's
+// configuration); feat says whether this launch writes them.
+template <class S, class P, class C, class M>
+constexpr bool has_feat_variant() {
+    return sizeof(S) == 4 && sizeof(P) == 4 && sizeof(C) == 4 && !M::kSutherland;
+}
+
 template <class S, class P, class C, class M, int FLUX, int EPB>
-cudaError_t launch_a(const StageAParams<S, P, C>& A, long long nelem, cudaStream_t s) {
+cudaError_t launch_a(const StageAParams<S, P, C>& A, long long nelem, cudaStream_t s, bool feat = false) {
     const unsigned grid = (unsigned)((nelem + EPB - 1) / EPB);
     if (grid == 0) return cudaSuccess;
     const size_t smem = sizeof(SlotA<P, C>) * EPB;
+    if constexpr (has_feat_variant<S, P, C, M>() && EPB == 4) {
+        if (feat) {
+            stage_a_kernel<S, P, C, M, FLUX, EPB, true><<<grid, LPE * EPB, smem, s>>>(A);
+            return cudaGetLastError();
+        }
+    }
+    if (feat) return cudaErrorInvalidValue;   // no variant writes the features for this launch
     stage_a_kernel<S, P, C, M, FLUX, EPB><<<grid, LPE * EPB, smem, s>>>(A);
     return cudaGetLastError();
 }
 
 template <class S, class P, class C, class M, int FLUX>
-cudaError_t launch_a_epb(const StageAParams<S, P, C>& A, long long nelem, int epb, cudaStream_t s) {
-    if (epb == 2) return launch_a<S, P, C, M, FLUX, 2>(A, nelem, s);
-    return launch_a<S, P, C, M, FLUX, 4>(A, nelem, s);
+cudaError_t launch_a_epb(const StageAParams<S, P, C>& A, long long nelem, int epb, cudaStream_t s, bool feat) {
+    if (epb == 2 && !feat) return launch_a<S, P, C, M, FLUX, 2>(A, nelem, s);
+    return launch_a<S, P, C, M, FLUX, 4>(A, nelem, s, feat);
 }
 
 template <class S, class P, class C, class M>
-cudaError_t launch_a_flux(const StageAParams<S, P, C>& A, int flux, long long nelem, int epb, cudaStream_t s) {
+cudaError_t launch_a_flux(const StageAParams<S, P, C>& A, int flux, long long nelem, int epb, cudaStream_t s,
+                          bool feat) {
     if (A.suth >= (C)0) {
-        // Sutherland variant: 4 elements per block only
+        // Sutherland variant: 4 elements per block only, no feature writing
+        if (feat) return cudaErrorInvalidValue;
         using MS = WithSutherland<M>;
         switch (flux) {
             case kSlau2: return launch_a<S, P, C, MS, kSlau2, 4>(A, nelem, s);
@@ -47,9 +64,9 @@ cudaError_t launch_a_flux(const StageAParams<S, P, C>& A, int flux, long long ne
         }
     }
     switch (flux) {
-        case kSlau2: return launch_a_epb<S, P, C, M, kSlau2>(A, nelem, epb, s);
-        case kAusmPlus: return launch_a_epb<S, P, C, M, kAusmPlus>(A, nelem, epb, s);
-        default: return launch_a_epb<S, P, C, M, kRusanov>(A, nelem, epb, s);
+        case kSlau2: return launch_a_epb<S, P, C, M, kSlau2>(A, nelem, epb, s, feat);
+        case kAusmPlus: return launch_a_epb<S, P, C, M, kAusmPlus>(A, nelem, epb, s, feat);
+        default: return launch_a_epb<S, P, C, M, kRusanov>(A, nelem, epb, s, feat);
     }
 }
 
@@ -75,7 +92,7 @@ constexpr bool has_fast_variant() { return sizeof(C) == 4; }
 
 template <class S, class P, class C>
 cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
-    StageAParams<S, P, C> A;
+    StageAParams<S, P, C> A{};
     A.u_in = (const S*)L.u_in;
     A.u0 = (const S*)L.u0;
     A.u_out = (S*)(L.rhs ? L.rhs : L.u_out);
@@ -103,17 +120,19 @@ cudaError_t launch_stage_t(const StageLaunch& L, cudaStream_t s) {
     A.flags = L.flags | (L.rhs ? kDeferRK : 0);
     A.e0 = L.e0;
     A.e1 = L.e1;
+    const bool feat = L.feat != nullptr;
+    if (feat) A.feat = *L.feat;
     const long long count = L.e1 - L.e0;
     cudaError_t err = cudaSuccess;
     if (L.phases & 1) {
         if (L.ev[0]) cudaEventRecord(L.ev[0], s);
         if constexpr (has_fast_variant<C>()) {
             if (L.fast_math)
-                err = launch_a_flux<S, P, C, MathFast>(A, L.flux, count, L.epb_a, s);
+                err = launch_a_flux<S, P, C, MathFast>(A, L.flux, count, L.epb_a, s, feat);
             else
-                err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, count, L.epb_a, s);
+                err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, count, L.epb_a, s, feat);
         } else {
-            err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, count, L.epb_a, s);
+            err = launch_a_flux<S, P, C, MathIeee>(A, L.flux, count, L.epb_a, s, feat);
         }
         if (err != cudaSuccess) return err;
         if (L.ev[1]) cudaEventRecord(L.ev[1], s);

@@ -53,6 +53,8 @@
 // C = float.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "od_launch.h"
 #include "od_physics.cuh"
 
@@ -332,7 +334,75 @@ struct StageAParams {
     int flags;
     int flux;           // scheme id, read when the kernel's FLUX is kFluxRuntime
     long long e0, e1;   // element range of this launch
+    StageFeatures feat; // the closure's features, written by the FEAT kernels (f32)
 };
+
+
+// P1b of phase A with the closure attached: the features of the element's
+// input state at the thread's four points (the same operations, in the same
+// order, as the closure's features kernel: x derivatives from the thread's
+// x-line, y / z derivatives from the x-lines of its k-plane / j-column),
+// staged as bf16 in the gradient rows (not written before P2) and stored in
+// the fused inference kernel's tile layout as 16-byte chunks.
+template <class PA, class P = typename PA::P_t, class C = typename PA::C_t>
+__device__ __forceinline__ void stage_a_features(const PA& A, SlotA<P, C>& sm, long long e, int l, int swz,
+                                                 bool live, const P (&qx)[NV][4]) {
+    const StageFeatures& fp = A.feat;
+    const int j = l & 3, k = l >> 2;
+    float d[4][3][4];   // [var][direction][point of the line]
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        float ly[4][4], lz[4][4];   // the x-lines (m, k) and (j, m), m = 0..3
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            ld4s(&sm.u[v][sw(4 * (m + 4 * k), swz)], ly[m]);
+            ld4s(&sm.u[v][sw(4 * (j + 4 * m), swz)], lz[m]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                sx += fp.D[i * 4 + m] * qx[v][m];
+                sy += fp.D[j * 4 + m] * ly[m][i];
+                sz += fp.D[k * 4 + m] * lz[m][i];
+            }
+            d[v][0][i] = sx * fp.jac[0];
+            d[v][1][i] = sy * fp.jac[1];
+            d[v][2][i] = sz * fp.jac[2];
+        }
+    }
+    __nv_bfloat16* st = reinterpret_cast<__nv_bfloat16*>(&sm.g[0][0]);   // [channel][64 points]
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int p = i + 4 * l;
+        const float ir = 1.0f / qx[0][i];
+        float ch[kFeatChan];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) ch[v] = qx[v][i];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) ch[5 + 3 * a + b] = (d[1 + a][b][i] - qx[1 + a][i] * ir * d[0][b][i]) * ir;
+#pragma unroll
+        for (int c = 0; c < kFeatChan; ++c)
+            st[c * 64 + p] =
+                __float2bfloat16_rn(fminf(fmaxf((ch[c] - fp.mean[c]) * fp.inv_scale[c], -kFeatClip), kFeatClip));
+    }
+    __syncthreads();
+    if (live) {
+        // tile (e / 128), channel c: a 128 x 64 block, row e % 128, 16-byte
+        // chunk kc at ((row / 8) * 1024 + kc * 128 + (row % 8) * 16) bytes
+        char* tile = reinterpret_cast<char*>(fp.X) + (size_t)(e >> 7) * (128 * 64 * 2 * kFeatChan);
+        const int r = (int)(e & 127);
+        for (int q8 = l; q8 < kFeatChan * 8; q8 += 16) {
+            const int c = q8 >> 3, kc = q8 & 7;
+            *reinterpret_cast<uint4*>(tile + (size_t)c * (128 * 64 * 2) + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16) =
+                *reinterpret_cast<const uint4*>(&st[c * 64 + 8 * kc]);
+        }
+    }
+    __syncthreads();   // the gradient rows are P2's from here
+}
 
 // Inviscid part of the face corrections at the two faces of a line. Each
 // face's interface flux F_I is solved once, by the element on its plus side
@@ -755,7 +825,7 @@ __device__ __forceinline__ void stage_a_update(const PA& A, SlotA<P, C>& sm, lon
 
 // One tile of phase A: EPB elements starting at A.e0 + tile * EPB, LPE
 // threads each. Called by every thread of the block (it synchronises).
-template <class M, int FLUX, int EPB, class PA>
+template <class M, int FLUX, int EPB, bool FEAT = false, class PA>
 __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_raw, long long tile) {
     using S = typename PA::S_t;
     using P = typename PA::P_t;
@@ -788,6 +858,7 @@ __device__ __forceinline__ void stage_a_tile(const PA& A, unsigned char* smem_ra
         st4s(&sm.u[v][sw(4 * l, swz)], qx[v]);
     }
     __syncthreads();
+    if constexpr (FEAT) stage_a_features(A, sm, ec, l, swz, live, qx);
 
     // ---- P2-P4: face values, gradient, interface fluxes per direction
     P tr[3][2][NV];   // own face values of this thread's lines (kept only for f32 state arithmetic)
@@ -870,10 +941,14 @@ constexpr int stage_a_min_blocks() {
     return 1;
 }
 
-template <class S, class P, class C, class M, int FLUX, int EPB>
+template <class S, class P, class C, class M, int FLUX, int EPB, bool FEAT = false>
 __global__ void __launch_bounds__(LPE * EPB, (stage_a_min_blocks<S, P, C, EPB>())) stage_a_kernel(const StageAParams<S, P, C> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    stage_a_tile<M, FLUX, EPB>(A, smem_raw, blockIdx.x);
+    // the closure network launched next may start its prologue (and prefetch
+    // its weights) on SMs this grid no longer needs; it reads the features
+    // and the RHS only after griddepcontrol.wait, i.e. after this grid
+    if constexpr (FEAT) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    stage_a_tile<M, FLUX, EPB, FEAT>(A, smem_raw, blockIdx.x);
 }
 
 template <class S, class P, class C>
