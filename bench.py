@@ -390,12 +390,24 @@ def run_closure_form(args, world, rank, local):
     if args.epochs:
         cfg["epochs"] = args.epochs
     log = lambda m: print(m, file=sys.stderr, flush=True)
-    data = CL.generate_data(cfg, device=local, log=log)
-    net, tr = CL.train(data, cfg, device=local, log=log)
-    alpha, cal = CL.calibrate(net, data, cfg, device=local, log=log)
-    norm = {"mean": data["mean"].tolist(), "scale": data["scale"].tolist(), "out_scale": data["out_scale"].tolist(),
-            "alpha": alpha, "calibration": [(a, e) for a, e in cal]}
-    del data
+    if args.load_weights:
+        # evaluation only, with a trained network (e.g. the shipped
+        # forms/closure_channel24.npz): no data generation, training or calibration
+        z = np.load(args.load_weights)
+        net = CL.Network(max_rows=nc ** 3)
+        net.set_params({k: z[k] for k in CL.NAMES})
+        alpha = float(z["alpha"])
+        net.set_scaling(z["mean"], z["scale"], alpha * z["out_scale"])
+        tr = {"history": [], "train_s": 0.0, "steps": 0}
+        norm = {"mean": z["mean"].tolist(), "scale": z["scale"].tolist(), "out_scale": z["out_scale"].tolist(),
+                "alpha": alpha, "weights": os.path.basename(args.load_weights)}
+    else:
+        data = CL.generate_data(cfg, device=local, log=log)
+        net, tr = CL.train(data, cfg, device=local, log=log)
+        alpha, cal = CL.calibrate(net, data, cfg, device=local, log=log)
+        norm = {"mean": data["mean"].tolist(), "scale": data["scale"].tolist(),
+                "out_scale": data["out_scale"].tolist(), "alpha": alpha, "calibration": [(a, e) for a, e in cal]}
+        del data
     torch.cuda.empty_cache()
     ev = CL.evaluate(net, cfg, device=local, log=log)
     if args.save_weights:
@@ -554,6 +566,7 @@ def main():
     ap.add_argument("--snaps", type=int, default=0, help="closure: snapshots per training seed (0 = 125)")
     ap.add_argument("--epochs", type=int, default=0, help="closure: training epochs (0 = 8)")
     ap.add_argument("--save-weights", default="", help="closure: write the trained network (.npz)")
+    ap.add_argument("--load-weights", default="", help="closure: evaluate this trained network (.npz) only")
     ap.add_argument("--slabs", type=int, default=4, help="slabs: number of z-slabs")
     args = ap.parse_args()
     if args.warmup < 3:
