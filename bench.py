@@ -278,13 +278,25 @@ def run_ours(args, world, rank, local):
     out = None
     if rank == 0:
         traffic = None
+        issue = None
         tpath = os.path.join(ROOT, "profiles", "stage_a_traffic.json")
         if os.path.exists(tpath):
             try:
                 with open(tpath) as fh:
-                    traffic = json.load(fh).get("bytes_per_launch")
+                    prof = json.load(fh)
+                traffic = prof.get("bytes_per_launch")
+                winst = prof.get("warp_instructions_per_launch")
+                if winst and args.physics == "reference":
+                    # the issue roofline phase A is bound by: its warp
+                    # instructions (ncu) over 148 SMs x 4 schedulers x the
+                    # sampled SM clock, one instruction per scheduler and cycle
+                    mhz = (clk or {}).get("sm_mhz") or 1965.0
+                    floor_ms = winst / (148 * 4 * mhz * 1e6) * 1e3
+                    issue = {"warp_instructions_per_launch": int(winst), "sm_mhz": mhz,
+                             "min_launch_ms_at_full_issue": round(floor_ms, 5),
+                             "frac": round(floor_ms / avg_a, 4)}
             except Exception:
-                traffic = None
+                traffic, issue = None, None
         metric = METRIC if args.physics == "reference" else METRIC[:-1] + ", Sutherland, Re_bulk 3000)"
         out = {
             "metric": metric, "value": round(value, 3), "unit": "Gdof*stage/s", "n_gpus": world,
@@ -301,7 +313,7 @@ def run_ours(args, world, rank, local):
                          "kernel": "od::stage_a_kernel (phase A, one launch per RK stage)",
                          "avg_launch_ms": round(avg_a, 5), "peak_kind": peak_kind,
                          "alg_bytes_per_launch": int(alg_bytes_launch),
-                         "phase_b_avg_ms": round(ms_b / n_st, 5)},
+                         "phase_b_avg_ms": round(ms_b / n_st, 5), "issue": issue},
             "gpu_launches": int(solver.launches_per_step * RK_PER_STEP * args.steps),
             "clocks": clk,
             "state_finite": finite,
