@@ -234,3 +234,37 @@ def test_dynamic_mode_wait_timeout_is_reported_and_recoverable():
         E.step(2)
         for k in range(len(BOXES)):
             _close(E.get_state(k), want[k])
+
+
+@pytest.mark.gpu
+def test_more_boxes_than_constant_memory_holds():
+    """Ensembles of more than 64 boxes read each box's parameters from global
+    memory (copied into shared memory per block) instead of constant memory:
+    the batched and persistent modes agree with the boxes alone; the dynamic
+    mode refuses them."""
+    from opendynamo_b200 import _native as N
+    boxes = []
+    for b in range(70):
+        flux = ("slau2", "rusanov", "ausm+")[b % 3]
+        boxes.append(Box((2, 1 + b % 2, 2), (2 * math.pi, 2.0, math.pi), flux, bool(b % 2), 1e-4 * (1 + b % 5),
+                         1e-3 * (b % 2), 5e-4 * (1 + b % 3)))
+    states = [random_smooth(*b.n, seed=200 + k, dtype=np.float32) for k, b in enumerate(boxes)]
+    check = [0, 1, 2, 66, 67, 68, 69]
+    want = _alone([boxes[k] for k in check], [states[k] for k in check], 2)
+    with Ensemble(boxes) as E:
+        results = {}
+        for mode in ("batched", "persistent"):
+            if mode == "persistent":
+                E.set_shape(4, 0, True)
+                assert E.info()["blocks_per_sm"] > 0
+            else:
+                assert E.info()["blocks_per_sm"] == BATCHED
+            for k, u in enumerate(states):
+                E.set_state(k, u)
+            E.step(2)
+            results[mode] = [E.get_state(k) for k in check]
+        with pytest.raises(N.OdError, match="at most 64 boxes"):
+            E.set_shape(4, DYNAMIC, True)
+    for i in range(len(check)):
+        _close(results["batched"][i], want[i])
+        _close(results["persistent"][i], want[i])
