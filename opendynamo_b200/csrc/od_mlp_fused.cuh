@@ -17,9 +17,9 @@
 // output layer runs as two passes of N = 160 (columns 0-159 and 160-319:
 // variables 0-2.5 and 2.5-5).
 //
-// Shared memory (197 KB): one 64 KB activation buffer of four 128 x 64
-// k-blocks, four 32 KB weight stages and the biases (the RHS update reduces
-// straight from registers). A layer's epilogue overwrites its own input in
+// Shared memory (197 KiB, 198 KiB with the alignment slack the launch adds):
+// one 64 KiB activation buffer of four 128 x 64 k-blocks, four 32 KiB weight
+// stages and the biases (the RHS update reduces straight from registers). A layer's epilogue overwrites its own input in
 // place: it starts only after all of the layer's MMAs have completed. During
 // layer 1 the activation buffer holds the feature stages instead (layer 1's
 // output is written after its last MMA). Tensor memory: 256 fp32 columns,
