@@ -548,11 +548,21 @@ int od_get_state_async(od_ctx* c, void* host, size_t bytes, void* stream) {
     if (int rc = set_device(c)) return rc;
     cudaError_t e = cudaSuccess;
     if (!c->snap) {
-        e = cudaMalloc(&c->snap, c->state_bytes);
+        void* buf = nullptr;
+        e = cudaMalloc(&buf, c->state_bytes);
+        if (e == cudaSuccess) c->snap = buf;
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_snap, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(c->ev_copied, c->stream);
-        if (e != cudaSuccess) return cuda_fail(c, e, "state snapshot buffer");
+        if (e != cudaSuccess) {
+            // leave nothing half made: the next call starts over
+            if (c->ev_copied) cudaEventDestroy(c->ev_copied);
+            if (c->ev_snap) cudaEventDestroy(c->ev_snap);
+            if (c->snap) cudaFree(c->snap);
+            c->ev_copied = c->ev_snap = nullptr;
+            c->snap = nullptr;
+            return cuda_fail(c, e, "state snapshot buffer");
+        }
     }
     cudaStream_t s = (cudaStream_t)stream;
     // the compute stream: wait until the previous download has read the
@@ -575,11 +585,21 @@ int od_set_state_async(od_ctx* c, const void* host, size_t bytes, void* stream) 
     if (int rc = set_device(c)) return rc;
     cudaError_t e = cudaSuccess;
     if (!c->stage) {
-        e = cudaMalloc(&c->stage, c->state_bytes);
+        void* buf = nullptr;
+        e = cudaMalloc(&buf, c->state_bytes);
+        if (e == cudaSuccess) c->stage = buf;
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_staged, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_taken, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(c->ev_taken, c->stream);
-        if (e != cudaSuccess) return cuda_fail(c, e, "state staging buffer");
+        if (e != cudaSuccess) {
+            // leave nothing half made: the next call starts over
+            if (c->ev_taken) cudaEventDestroy(c->ev_taken);
+            if (c->ev_staged) cudaEventDestroy(c->ev_staged);
+            if (c->stage) cudaFree(c->stage);
+            c->ev_taken = c->ev_staged = nullptr;
+            c->stage = nullptr;
+            return cuda_fail(c, e, "state staging buffer");
+        }
     }
     cudaStream_t s = (cudaStream_t)stream;
     // the caller's stream: once the previous upload has been taken over,
