@@ -141,7 +141,9 @@ struct od_ctx {
     // launch shape: 4 elements per phase-A block; phase B with a thread per
     // (element, variable, x-line), 2 elements per block (B200, 48^3 f32: phase
     // B 0.122 ms against 0.128 with a thread per x-line and 8 elements, 0.136
-    // with 16; phase A 2 vs 4 equal)
+    // with 16; phase A 2 vs 4 equal, 8 and 16 slower: 262.6 and 274.9 against
+    // 260.4 us, the larger blocks' barriers cost more than their warps gain
+    // from running close together in the code)
     int epb_a = 4, epb_b = 2;
     std::string err;
     bool timing = false;
