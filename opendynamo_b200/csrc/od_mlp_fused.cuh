@@ -90,7 +90,7 @@ __device__ __forceinline__ uint32_t fused_w_bytes(int s) { return s < 22 ? kFSta
 
 constexpr uint32_t kFXBytes = BM * BK * 2;   // feature block of a layer-1 step
 
-// thread 0: the weight tile of step s (and for layer 1 the tile's feature
+// The producer's lane 0: the weight tile of step s (and for layer 1 the tile's feature
 // block) into its stage, bulk copies that complete on the stage's `full`
 // barrier. with_x = false posts the barrier's byte count for both but copies
 // only the weights; fused_load_x then adds the features.
