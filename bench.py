@@ -129,6 +129,16 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _tensor_peak():
+    """Dense bf16 TFLOP/s: the measured burst figure, else the fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def bench_config(world: int = 1) -> dict:
     """The workload description both arms (ours and --impl reference) print."""
     w = WORKLOAD
@@ -465,7 +475,12 @@ def run_closure_step(args, world, rank, local):
     """Cost of the learned closure inside the step: the coarse channel (24^3 by
     default) stepped with and without the network attached (random weights,
     output scaled to 1e-6 so the flow stays the plain one). CUDA events on the
-    solver's stream."""
+    solver's stream. A second run of each with per-stage events splits the
+    stage: phase A (with the features) and the rest (network + phase B with
+    the closure, phase B alone without). The network's time is estimated as
+    the difference of the rests; the events between the launches also stop
+    the network from starting in phase A's tail, so the estimate is an upper
+    bound of the network's share of the step."""
     if rank != 0:
         return None
     import torch
@@ -492,15 +507,34 @@ def run_closure_step(args, world, rank, local):
             s.step(args.warmup, float(np.float32(dt)))
             s.sync()
             out[name] = CL._timed_steps(s, steps, dt) / steps
+            s.set_timing(True)
+            s.step(steps, float(np.float32(dt)))
+            ms_a, ms_rest, n_st = s.timing()
+            s.set_timing(False)
+            out[name + "_stage_us"] = (ms_a / n_st * 1e3, ms_rest / n_st * 1e3)
     net.close()
     npts = n ** 3 * 64
+    # one network launch per stage: every element through 896 -> 256 -> 256 -> 256 -> 320
+    flop = n ** 3 * 2.0 * (896 * 256 + 2 * 256 * 256 + 256 * 320)
+    net_us = out["closure_stage_us"][1] - out["plain_stage_us"][1]
+    peak, peak_kind = _tensor_peak()
+    achieved = flop / (net_us * 1e-6) / 1e12 if net_us > 0 else None
     return {"metric": f"closure step cost, channel {n}^3 (ms per SSP-RK3 step)", "value": round(out["closure"], 4),
             "unit": "ms/step", "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": False,
             "dtype": "f32 solver / bf16 network", "data": "synthetic (channel trip IC, random network)",
             "config": {"workload": f"channel {n}^3, SLAU2, per-stage features + fused tcgen05 network kernel",
                        "form": "closure-step"},
             "plain_ms_per_step": round(out["plain"], 4),
-            "closure_gdof_stage_s": round(npts * 3 / (out["closure"] / 1e3) / 1e9, 3)}
+            "closure_gdof_stage_s": round(npts * 3 / (out["closure"] / 1e3) / 1e9, 3),
+            "stage_us": {"closure": {"phase_a_with_features": round(out["closure_stage_us"][0], 2),
+                                     "network_and_phase_b": round(out["closure_stage_us"][1], 2)},
+                         "plain": {"phase_a": round(out["plain_stage_us"][0], 2),
+                                   "phase_b": round(out["plain_stage_us"][1], 2)}},
+            "roofline": {"bound": "tensor", "kernel": "od::mlp::mlp_fused_kernel (one launch per RK stage)",
+                         "flop_per_launch": flop, "launch_us_estimate": round(net_us, 2),
+                         "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "TFLOP/s",
+                         "frac": round(achieved / peak, 4) if achieved else None, "peak_kind": peak_kind,
+                         "how": "network + phase B with the closure minus phase B without it, per stage"}}
 
 
 def run_slabs_form(args, world, rank, local):
