@@ -251,7 +251,7 @@ int upload_constants(refh* h) {
 struct Scalar {
     double d;
     float f;
-    void set(bool c64, double v) {
+    void set(double v) {
         d = v;
         f = (float)v;
     }
@@ -267,9 +267,9 @@ int rhs_stage(refh* h) {
     const bool c64 = h->p.c_f64;
     int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
     Scalar lx, ly, lz;
-    lx.set(c64, c64 ? (double)h->p.lx : (double)(float)h->p.lx);
-    ly.set(c64, c64 ? (double)h->p.ly : (double)(float)h->p.ly);
-    lz.set(c64, c64 ? (double)h->p.lz : (double)(float)h->p.lz);
+    lx.set(c64 ? (double)h->p.lx : (double)(float)h->p.lx);
+    ly.set(c64 ? (double)h->p.ly : (double)(float)h->p.ly);
+    lz.set(c64 ? (double)h->p.lz : (double)(float)h->p.lz);
     void* av[] = {&h->u, &h->rhs, &h->sl[0], &h->sl[1], &h->sl[2], &h->sl[3], &h->sl[4], &h->sl[5],
                   &nx, &ny, &nz, lx.ptr(c64), ly.ptr(c64), lz.ptr(c64)};
     if (int r = launch(h, h->k_vol, (unsigned)h->nelem, 64, av, "volume")) return r;
@@ -289,12 +289,12 @@ int rk_stage(refh* h, bool stage1, CUdeviceptr dst, CUdeviceptr src, double a, d
     int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
     int size = (int)h->state_size;
     Scalar lx, ly, lz, sa, sb, sc;
-    lx.set(c64, h->p.lx);
-    ly.set(c64, h->p.ly);
-    lz.set(c64, h->p.lz);
-    sa.set(c64, a);
-    sb.set(c64, b);
-    sc.set(c64, c);
+    lx.set(h->p.lx);
+    ly.set(h->p.ly);
+    lz.set(h->p.lz);
+    sa.set(a);
+    sb.set(b);
+    sc.set(c);
     // cudarc LaunchConfig::for_num_elems: 1024 threads per block (h->rk_block,
     // lower only where the kernel cannot launch 1024 threads on this GPU)
     unsigned n4 = (unsigned)(h->state_size / 4);
