@@ -12,18 +12,19 @@
 // streamed, in 64-wide K blocks, four stages deep, as bulk copies that
 // complete on the stage's `full` mbarrier.
 //
-// Warp roles: one producer warp (lane 0 issues the copies and tcgen05.mma,
-// kind::f16, M = 128, K = 16, and commits each stage's MMAs to its `bar`
-// mbarrier and each layer's last MMAs to a `done` mbarrier) and 16 epilogue
-// warps (warp w: TMEM lanes 32 (w % 4) .. +31). The layers alternate between
-// two accumulators of 256 TMEM columns, so a layer's MMAs never wait for the
-// epilogue of the layer before to finish reading its accumulator. A hidden
-// layer's epilogue runs k-block by k-block (64 columns; each warp 16 of
-// them) and releases each k-block of the next layer's input on a `kready`
-// mbarrier, so the next layer's MMAs start on the first k-block while the
-// epilogue works on the rest. The output layer runs as two passes of
-// N = 160 (columns 0-159 and 160-319: variables 0-2.5 and 2.5-5), the first
-// pass's epilogue beside the second pass's MMAs.
+// Warp roles: a load warp (lane 0 issues the bulk copies, a stage ahead of
+// the MMAs as soon as the stage's MMAs are complete), an MMA warp (lane 0
+// issues tcgen05.mma, kind::f16, M = 128, K = 16, and commits each stage's
+// MMAs to its `bar` mbarrier and each layer's last MMAs to a `done`
+// mbarrier) and 16 epilogue warps (warp w: TMEM lanes 32 (w % 4) .. +31). The
+// layers alternate between two accumulators of 256 TMEM columns, so a
+// layer's MMAs never wait for the epilogue of the layer before to finish
+// reading its accumulator. A hidden layer's epilogue runs k-block by k-block
+// (64 columns; each warp 16 of them) and releases each k-block of the next
+// layer's input on a `kready` mbarrier, so the next layer's MMAs start on the
+// first k-block while the epilogue works on the rest. The output layer runs
+// as two passes of N = 160 (columns 0-159 and 160-319: variables 0-2.5 and
+// 2.5-5), the first pass's epilogue beside the second pass's MMAs.
 //
 // Shared memory (197 KiB, 198 KiB with the alignment slack the launch adds):
 // one 64 KiB activation buffer of four 128 x 64 k-blocks, four 32 KiB weight
@@ -45,7 +46,7 @@ namespace mlp {
 constexpr int kFIn = 896, kFHid = 256, kFOut = 320, kFPass = 160;
 constexpr int kFStages = 4;
 constexpr int kFEpiThreads = 512;   // 16 epilogue warps: warp w reads TMEM lanes 32 (w % 4) .. +31
-constexpr int kFThreads = kFEpiThreads + 32;   // + the producer warp
+constexpr int kFThreads = kFEpiThreads + 64;   // + the MMA warp and the load warp
 constexpr int kFGroups = kFEpiThreads / 128;   // column groups of the output epilogue
 constexpr int kFUnits = 5;   // hidden layers 1-3, output passes 0 and 1
 constexpr int kFSteps = kFIn / BK + 2 * (kFHid / BK) + 2 * (kFHid / BK);   // 14 + 4 + 4 + 2 x 4 = 30
@@ -90,7 +91,7 @@ __device__ __forceinline__ uint32_t fused_w_bytes(int s) { return s < 22 ? kFSta
 
 constexpr uint32_t kFXBytes = BM * BK * 2;   // feature block of a layer-1 step
 
-// The producer's lane 0: the weight tile of step s (and for layer 1 the tile's feature
+// The load warp's lane 0: the weight tile of step s (and for layer 1 the tile's feature
 // block) into its stage, bulk copies that complete on the stage's `full`
 // barrier. with_x = false posts the barrier's byte count for both but copies
 // only the weights; fused_load_x then adds the features.
@@ -231,22 +232,44 @@ __device__ __forceinline__ void fused_fail(const FusedArgs& g, FusedSmem& sm) {
 
 __device__ __forceinline__ bool fused_failed(FusedSmem& sm) { return *(volatile int*)&sm.failed != 0; }
 
-// Producer (lane 0 of the last warp): the bulk copies and the MMAs of every
-// step, in step order. A hidden layer's or output pass's step kb waits for
-// k-block kb of the layer before (kready); every step waits for its stage.
-__device__ __forceinline__ void fused_producer(const FusedArgs& g, FusedSmem& sm, uint32_t tmem) {
-    int w_issued = 0, w_landed = 0;   // stage fills requested / seen complete
-    int last_mma = -1;                // last step whose MMAs were issued
+// Load warp (its lane 0): the bulk copies of every step, kFStages steps ahead
+// of the MMAs. Step s reuses the stage of step s - kFStages once that step's
+// MMAs are complete (its `bar` commit).
+__device__ __forceinline__ void fused_loader(const FusedArgs& g, FusedSmem& sm) {
+    int issued = 0;
     // The weights and biases do not depend on the kernel launched before this
     // one (phase A or the features kernel, which may let this kernel start
     // early): the first weight tiles are requested before waiting for it, the
     // features after.
-    for (int i = 0; i < kFStages - 1; ++i) {
+    for (int i = 0; i < kFStages; ++i) {
         fused_load(g, sm, i, blockIdx.x, false);
-        ++w_issued;
+        ++issued;
     }
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    for (int i = 0; i < kFStages - 1; ++i) fused_load_x(g, sm, i, blockIdx.x);
+    for (int i = 0; i < kFStages; ++i) fused_load_x(g, sm, i, blockIdx.x);
+    for (int s = kFStages; s < kFSteps && !fused_failed(sm); ++s) {
+        if (!mbar_wait(smem_addr(&sm.bar[s % kFStages]), (uint32_t)((s / kFStages - 1) & 1))) {
+            fused_fail(g, sm);
+            break;
+        }
+        fused_load(g, sm, s, blockIdx.x);
+        ++issued;
+    }
+    // before the CTA frees its memory no copy may still be writing it: wait
+    // for the last fill of every stage (they have landed already unless a
+    // wait failed)
+    for (int s = issued - kFStages; s < issued; ++s)
+        if (s >= 0 && !mbar_wait(smem_addr(&sm.full[s % kFStages]), (uint32_t)((s / kFStages) & 1)))
+            fused_fail(g, sm);
+}
+
+// MMA warp (its lane 0): the tcgen05.mma of every step in step order. A
+// hidden layer's or output pass's step kb waits for k-block kb of the layer
+// before (kready); every step waits for its stage (full). Each step's MMAs
+// are committed to the stage's `bar` (stage free) and a layer's last ones
+// also to `done` (accumulator complete).
+__device__ __forceinline__ void fused_mma(const FusedArgs& g, FusedSmem& sm, uint32_t tmem) {
+    int last_mma = -1;   // last step whose MMAs were issued
     for (int s = 0; s < kFSteps && !fused_failed(sm); ++s) {
         const FStep f = fused_step(s);
         const int u = fused_unit(f);
@@ -262,7 +285,6 @@ __device__ __forceinline__ void fused_producer(const FusedArgs& g, FusedSmem& sm
             fused_fail(g, sm);
             break;
         }
-        ++w_landed;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int n = f.layer == 3 ? kFPass : kFHid;
         const uint32_t idesc = instr_desc(BM, n);
@@ -284,26 +306,13 @@ __device__ __forceinline__ void fused_producer(const FusedArgs& g, FusedSmem& sm
                          smem_addr(&sm.bar[st]))
                      : "memory");
         last_mma = s;
-        const bool last = s + 1 == kFSteps || fused_step(s + 1).kb == 0;
-        if (last)
+        if (s + 1 == kFSteps || fused_step(s + 1).kb == 0)
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_addr(&sm.done[u & 1]))
                          : "memory");
-        // refill the stage of step s-1 with step s+kFStages-1 once its MMAs are done
-        const int ns = s + kFStages - 1;
-        if (ns < kFSteps) {
-            if (s >= 1 && !mbar_wait(smem_addr(&sm.bar[ns % kFStages]), (uint32_t)(((s - 1) / kFStages) & 1))) {
-                fused_fail(g, sm);
-                break;
-            }
-            fused_load(g, sm, ns, blockIdx.x);
-            ++w_issued;
-        }
     }
-    // before the CTA frees its memory: no copy may still be writing its shared
-    // memory and no MMA still running (both only after a failed wait)
-    for (int s = w_landed; s < w_issued; ++s)
-        if (!mbar_wait(smem_addr(&sm.full[s % kFStages]), (uint32_t)((s / kFStages) & 1))) fused_fail(g, sm);
+    // no MMA may still be running when the CTA frees its tensor memory (only
+    // after a failed wait has no epilogue waited for the last ones)
     if (last_mma >= 0 &&
         !mbar_wait(smem_addr(&sm.bar[last_mma % kFStages]), (uint32_t)((last_mma / kFStages) & 1)))
         fused_fail(g, sm);
@@ -341,7 +350,10 @@ __global__ void __launch_bounds__(kFThreads, 1) mlp_fused_kernel(const FusedArgs
     const uint32_t tmem = sm.tmem_base;
 
     if (warp == kFEpiThreads / 32) {
-        if ((t & 31) == 0) fused_producer(g, sm, tmem);
+        if ((t & 31) == 0) fused_mma(g, sm, tmem);
+        __syncwarp();
+    } else if (warp == kFEpiThreads / 32 + 1) {
+        if ((t & 31) == 0) fused_loader(g, sm);
         __syncwarp();
     } else {
         // the RHS the output epilogues add to is written by the kernel before
