@@ -103,6 +103,14 @@ def run(tiles_a, tiles_b, grid, launches, seed):
         assert counter[0] == (launch + 1) * per
 
 
+def test_model_chunk_matches_the_kernel():
+    import os
+    import re
+    src = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "opendynamo_b200", "csrc",
+                            "od_ensemble.cu")).read()
+    assert int(re.search(r"constexpr int kDynChunk = (\d+);", src).group(1)) == CHUNK
+
+
 @pytest.mark.parametrize("seed", range(12))
 def test_dynamic_mode_random_boxes(seed):
     rng = random.Random(100 + seed)

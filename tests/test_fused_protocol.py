@@ -188,6 +188,19 @@ def run(seed, n_epi=4, limit=200_000, load=loader, issue=mma):
     assert all(b.phases == 3 for b in k.kready)
 
 
+def test_model_constants_match_the_kernel():
+    """The model's stage count and step counts are the kernel's."""
+    import os
+    import re
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "opendynamo_b200", "csrc")
+    fused = open(os.path.join(csrc, "od_mlp_fused.cuh")).read()
+    mlp = open(os.path.join(csrc, "od_mlp.cuh")).read()
+    stages = int(re.search(r"constexpr int kFStages = (\d+);", fused).group(1))
+    k_in, k_hid = (int(x) for x in re.search(r"constexpr int kFIn = (\d+), kFHid = (\d+)", fused).groups())
+    bk = int(re.search(r"constexpr int BK = (\d+);", mlp).group(1))
+    assert (K_STAGES, STEPS_L1, STEPS_H) == (stages, k_in // bk, k_hid // bk)
+
+
 @pytest.mark.parametrize("seed", range(40))
 def test_fused_kernel_protocol_random_interleavings(seed):
     run(seed, n_epi=1 + seed % 4)
