@@ -12,8 +12,9 @@
 // streamed, in 64-wide K blocks, four stages deep, as bulk copies that
 // complete on the stage's `full` mbarrier.
 //
-// Warp roles: a load warp (lane 0 issues the bulk copies, a stage ahead of
-// the MMAs as soon as the stage's MMAs are complete), an MMA warp (lane 0
+// Warp roles: a load warp (lane 0 issues the bulk copies, refilling each
+// stage as soon as its MMAs are complete, up to four steps ahead of the
+// MMAs), an MMA warp (lane 0
 // issues tcgen05.mma, kind::f16, M = 128, K = 16, and commits each stage's
 // MMAs to its `bar` mbarrier and each layer's last MMAs to a `done`
 // mbarrier) and 16 epilogue warps (warp w: TMEM lanes 32 (w % 4) .. +31). The
